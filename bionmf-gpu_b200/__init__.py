@@ -1,0 +1,257 @@
+"""nmf-b200: B200-native KL-NMF engine (drop-in for NMF-mGPU's single-GPU path).
+
+Python host binding over the C ABI in ``include/nmfb200.h`` (``libnmfb200.so``,
+built in-tree for sm_100a).  It mirrors the reference's entry points
+(src/NMF_routines.c, src/NMF_GPU.c):
+
+====================  ==========================================
+reference             here
+====================  ==========================================
+init_V + upload       ``NMF(V, k)`` / ``NMF.set_V``
+init_random (CPU)     ``NMF.init_random(seed)``
+update_H / update_W   ``NMF.update_H()`` / ``NMF.update_W()``
+matrix_adjust         ``NMF.adjust()``
+get_classification    ``NMF.classification()``
+nmf()                 ``NMF.run(n_iters, niter_test_conv, stop_threshold)``
+dot_product_VWH       ``NMF.dot_product_VWH()``
+====================  ==========================================
+
+There is no CPU fallback: if the shared library is missing or no sm_100
+device is present, constructing an ``NMF`` raises ``NMFError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnmfb200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "nmfb200.h")
+
+ARM_FUSED = 0
+ARM_PLAIN = 1
+ARM_FUSED_TF32 = 2
+ARMS = {"fused": ARM_FUSED, "plain": ARM_PLAIN, "fused_tf32": ARM_FUSED_TF32}
+
+NMFB_OK = 0
+_ERRNAMES = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENODEV", -5: "ESTATE", -6: "ETIMEOUT"}
+
+
+class NMFError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libnmfb200.so and declare every exported function."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise NMFError(-4, f"{path} is missing: build it with __graft_entry__.build() (no CPU fallback)")
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    u32, sz, i32 = C.c_uint32, C.c_size_t, C.c_int
+    fp = C.POINTER(C.c_float)
+    sig = {
+        "nmfb_version": ([], C.c_char_p),
+        "nmfb_device_count": ([], i32),
+        "nmfb_create": ([C.POINTER(vp), i32, u32, u32, u32, i32], i32),
+        "nmfb_destroy": ([vp], i32),
+        "nmfb_last_error": ([vp], C.c_char_p),
+        "nmfb_set_arm": ([vp, i32], i32),
+        "nmfb_set_V": ([vp, fp, sz], i32),
+        "nmfb_set_V_device": ([vp, vp, sz], i32),
+        "nmfb_init_random": ([vp, u32], i32),
+        "nmfb_set_WH": ([vp, fp, sz, fp, sz], i32),
+        "nmfb_update_H": ([vp], i32),
+        "nmfb_update_W": ([vp], i32),
+        "nmfb_adjust": ([vp], i32),
+        "nmfb_get_classification": ([vp, C.POINTER(u32)], i32),
+        "nmfb_run": ([vp, u32, u32, u32, C.POINTER(u32), C.POINTER(i32)], i32),
+        "nmfb_get_W": ([vp, fp, sz], i32),
+        "nmfb_get_H": ([vp, fp, sz], i32),
+        "nmfb_dot_product_VWH": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], i32),
+        "nmfb_kl_divergence": ([vp, C.POINTER(C.c_double)], i32),
+        "nmfb_device_factors": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u32)], i32),
+        "nmfb_device_V": ([vp, C.POINTER(vp), C.POINTER(sz)], i32),
+        "nmfb_set_stream": ([vp, vp], i32),
+        "nmfb_profile": ([vp, i32], i32),
+        "nmfb_profile_read": ([vp, i32, C.POINTER(C.c_double), C.POINTER(u32)], i32),
+        "nmfb_synchronize": ([vp], i32),
+        "nmfb_launch_count": ([vp], C.c_uint64),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def device_count() -> int:
+    return int(load_library().nmfb_device_count())
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class NMF:
+    """One factorisation V (n x m) ~ W (n x k) H (k x m) on one B200.
+
+    H is exchanged as the reference stores it: m rows of k factors.
+    """
+
+    def __init__(self, n: int, m: int, k: int, arm: str | int = "fused", device: int = 0):
+        L = load_library()
+        self._L = L
+        self.n, self.m, self.k = int(n), int(m), int(k)
+        self.arm = ARMS[arm] if isinstance(arm, str) else int(arm)
+        h = C.c_void_p()
+        rc = L.nmfb_create(C.byref(h), device, self.n, self.m, self.k, self.arm)
+        self._h = h
+        if rc != NMFB_OK:
+            msg = L.nmfb_last_error(h).decode() if h else "allocation failed"
+            L.nmfb_destroy(h)
+            self._h = None
+            raise NMFError(rc, msg)
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != NMFB_OK:
+            raise NMFError(rc, self._L.nmfb_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.nmfb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- reference entry points -------------------------------------------
+    def set_arm(self, arm):
+        self.arm = ARMS[arm] if isinstance(arm, str) else int(arm)
+        self._check(self._L.nmfb_set_arm(self._h, self.arm))
+
+    def set_V(self, V: np.ndarray):
+        V = np.ascontiguousarray(V, dtype=np.float32)
+        assert V.shape == (self.n, self.m), (V.shape, self.n, self.m)
+        self._check(self._L.nmfb_set_V(self._h, _fptr(V), self.m))
+
+    def set_V_device(self, ptr: int, ld: int):
+        self._check(self._L.nmfb_set_V_device(self._h, C.c_void_p(ptr), ld))
+
+    def init_random(self, seed: int):
+        self._check(self._L.nmfb_init_random(self._h, seed))
+
+    def set_WH(self, W: np.ndarray, H: np.ndarray):
+        W = np.ascontiguousarray(W, np.float32)
+        H = np.ascontiguousarray(H, np.float32)
+        assert W.shape == (self.n, self.k) and H.shape == (self.m, self.k)
+        self._check(self._L.nmfb_set_WH(self._h, _fptr(W), self.k, _fptr(H), self.k))
+
+    def update_H(self):
+        self._check(self._L.nmfb_update_H(self._h))
+
+    def update_W(self):
+        self._check(self._L.nmfb_update_W(self._h))
+
+    def adjust(self):
+        self._check(self._L.nmfb_adjust(self._h))
+
+    def classification(self) -> np.ndarray:
+        out = np.empty(self.m, np.uint32)
+        self._check(self._L.nmfb_get_classification(self._h, out.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return out
+
+    def run(self, n_iters=2000, niter_test_conv=10, stop_threshold=40):
+        it = C.c_uint32()
+        conv = C.c_int()
+        self._check(self._L.nmfb_run(self._h, n_iters, niter_test_conv, stop_threshold, C.byref(it), C.byref(conv)))
+        return int(it.value), bool(conv.value)
+
+    @property
+    def W(self) -> np.ndarray:
+        out = np.empty((self.n, self.k), np.float32)
+        self._check(self._L.nmfb_get_W(self._h, _fptr(out), self.k))
+        return out
+
+    @property
+    def H(self) -> np.ndarray:
+        out = np.empty((self.m, self.k), np.float32)
+        self._check(self._L.nmfb_get_H(self._h, _fptr(out), self.k))
+        return out
+
+    def dot_product_VWH(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(self._L.nmfb_dot_product_VWH(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def distance(self) -> float:
+        """The reference's final line: sqrt(||V-WH||^2) / sqrt(||V||^2)."""
+        a, b = self.dot_product_VWH()
+        return float(np.sqrt(b) / np.sqrt(a))
+
+    def kl_divergence(self) -> float:
+        d = C.c_double()
+        self._check(self._L.nmfb_kl_divergence(self._h, C.byref(d)))
+        return d.value
+
+    def device_factors(self):
+        w, h, ld = C.c_void_p(), C.c_void_p(), C.c_uint32()
+        self._check(self._L.nmfb_device_factors(self._h, C.byref(w), C.byref(h), C.byref(ld)))
+        return w.value, h.value, ld.value
+
+    def device_V(self):
+        v, ld = C.c_void_p(), C.c_size_t()
+        self._check(self._L.nmfb_device_V(self._h, C.byref(v), C.byref(ld)))
+        return v.value, ld.value
+
+    def set_stream(self, stream_handle: int | None):
+        """Queue work on an external CUDA stream (``torch.cuda.Stream().cuda_stream``)."""
+        self._check(self._L.nmfb_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def profile(self, enable: bool = True):
+        self._check(self._L.nmfb_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self, cls: int):
+        """(total_ms, launches) of kernel class cls: 0/1 = update_H/W main kernel, 2/3 = whole update."""
+        ms, cnt = C.c_double(), C.c_uint32()
+        self._check(self._L.nmfb_profile_read(self._h, cls, C.byref(ms), C.byref(cnt)))
+        return ms.value, int(cnt.value)
+
+    def synchronize(self):
+        self._check(self._L.nmfb_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        return int(self._L.nmfb_launch_count(self._h))
+
+
+def nmf_gpu(V: np.ndarray, k: int = 2, n_iters: int = 2000, niter_test_conv: int = 10, stop_threshold: int = 40,
+            seed: int = 3, arm: str = "fused", device: int = 0):
+    """One call equivalent of ``NMF_GPU <file> -k K -i I -j J -t T`` (CPU_RANDOM init).
+
+    Returns (W, H, iterations, converged, distance)."""
+    V = np.ascontiguousarray(V, np.float32)
+    with NMF(V.shape[0], V.shape[1], k, arm=arm, device=device) as e:
+        e.set_V(V)
+        e.init_random(seed)
+        it, conv = e.run(n_iters, niter_test_conv, stop_threshold)
+        return e.W, e.H, it, conv, e.distance()

@@ -1,0 +1,553 @@
+// nmfb_api.cu -- the C ABI of include/nmfb200.h: context life cycle, data
+// movement, the nmf() iteration loop with device-side convergence test.
+#include "nmfb_internal.cuh"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <new>
+
+using nmfb::ConvState;
+
+#define NMFB_VERSION "nmfb200 0.1 (sm_100a)"
+
+namespace {
+
+uint32_t padded_rank(uint32_t k)
+{
+    if (k <= 16) return 16;
+    return ((k + 31u) / 32u) * 32u;
+}
+
+int check_ctx(nmfb_ctx *ctx)
+{
+    if (!ctx) return NMFB_EINVAL;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "cudaSetDevice(%d): %s", ctx->device, cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+template <class T>
+int dev_alloc(nmfb_ctx *ctx, T **p, size_t items, const char *what)
+{
+    *p = nullptr;
+    if (items == 0) items = 1;
+    cudaError_t e = cudaMalloc((void **)p, items * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return nmfb_fail(ctx, NMFB_ENOMEM, "cudaMalloc(%s, %zu bytes): %s", what, items * sizeof(T),
+                         cudaGetErrorString(e));
+    }
+    return NMFB_OK;
+}
+
+void free_all(nmfb_ctx *ctx)
+{
+    void *bufs[] = {ctx->dV,   ctx->dW,    ctx->dH,     ctx->dAccW,  ctx->dAccH,  ctx->dWH,    ctx->dPart,
+                    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->dWhi, ctx->dWlo, ctx->dHhi,
+                    ctx->dHlo, ctx->dLabels, ctx->dFirst, ctx->dLastRep, ctx->dState};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (ctx->hState) cudaFreeHost(ctx->hState);
+    nmfb_fused_release(ctx);
+    for (int c = 0; c < 4; c++) {
+        if (!ctx->prof_ev[c]) continue;
+        for (int i = 0; i < 2 * NMFB_PROF_POOL; i++) cudaEventDestroy(ctx->prof_ev[c][i]);
+        free(ctx->prof_ev[c]);
+    }
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+}
+
+// Upload a host (rows x cols, ld) float matrix into a device rows x kp buffer
+// with zero padding, through a pinned staging buffer.
+int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, uint32_t cols, size_t ld)
+{
+    size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
+    float *stage = nullptr;
+    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&stage, bytes));
+    for (uint32_t r = 0; r < rows; r++) {
+        float *d = stage + (size_t)r * ctx->kp;
+        memcpy(d, src + (size_t)r * ld, cols * sizeof(float));
+        for (uint32_t c = cols; c < ctx->kp; c++) d[c] = 0.0f;
+    }
+    cudaError_t e = cudaMemcpyAsync(dst, stage, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFreeHost(stage);
+    if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "upload: %s", cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, size_t ld)
+{
+    size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
+    float *stage = nullptr;
+    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&stage, bytes));
+    cudaError_t e = cudaMemcpyAsync(stage, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess)
+        for (uint32_t r = 0; r < rows; r++) memcpy(dst + (size_t)r * ld, stage + (size_t)r * ctx->kp, ctx->k * sizeof(float));
+    cudaFreeHost(stage);
+    if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "download: %s", cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+int refresh_splits(nmfb_ctx *ctx)
+{
+    if (!ctx->dWhi) return NMFB_OK;
+    int rc = nmfb_split_tf32(ctx, ctx->dW, ctx->n, ctx->dWhi, ctx->dWlo);
+    if (rc) return rc;
+    return nmfb_split_tf32(ctx, ctx->dH, ctx->m, ctx->dHhi, ctx->dHlo);
+}
+
+int do_update_H(nmfb_ctx *ctx, int adjust)
+{
+    if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_H(ctx, adjust);
+    return nmfb_fused_update_H(ctx, adjust);
+}
+
+int do_update_W(nmfb_ctx *ctx, int adjust)
+{
+    if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_W(ctx, adjust);
+    return nmfb_fused_update_W(ctx, adjust);
+}
+
+int ready(nmfb_ctx *ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ctx->v_set) return nmfb_fail(ctx, NMFB_ESTATE, "V has not been set (nmfb_set_V)");
+    if (!ctx->wh_set) return nmfb_fail(ctx, NMFB_ESTATE, "W/H have not been initialised");
+    return NMFB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *nmfb_version(void) { return NMFB_VERSION; }
+
+int nmfb_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int usable = 0;
+    for (int d = 0; d < n; d++) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) == cudaSuccess && major == 10) usable++;
+    }
+    return usable;
+}
+
+int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, int arm)
+{
+    if (!out) return NMFB_EINVAL;
+    *out = nullptr;
+    nmfb_ctx *ctx = new (std::nothrow) nmfb_ctx;
+    if (!ctx) return NMFB_ENOMEM;
+    memset(ctx, 0, sizeof(*ctx));
+    ctx->device = device;
+    ctx->arm = arm;
+    *out = ctx;  // returned even on failure so that nmfb_last_error works; caller destroys it
+    if (n < 2 || m < 2) return nmfb_fail(ctx, NMFB_EINVAL, "both matrix dimensions must be greater than 1 (n=%u, m=%u)", n, m);
+    if (k < 2) return nmfb_fail(ctx, NMFB_EINVAL, "invalid factorization rank: K=%u (must be >= 2)", k);
+    if (k > (n < m ? n : m))
+        return nmfb_fail(ctx, NMFB_EINVAL,
+                         "invalid factorization rank: K=%u. It must not be greater than any of matrix dimensions.", k);
+    if (k > 256) return nmfb_fail(ctx, NMFB_EINVAL, "factorization rank K=%u exceeds the supported maximum of 256", k);
+    if (arm != NMFB_ARM_FUSED && arm != NMFB_ARM_PLAIN && arm != NMFB_ARM_FUSED_TF32)
+        return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return nmfb_fail(ctx, NMFB_ENODEV, "no CUDA device %d (devices: %d)", device, ndev);
+    }
+    cudaDeviceProp prop;
+    NMFB_CUDA_TRY(ctx, cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return nmfb_fail(ctx, NMFB_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a only", device,
+                         prop.major, prop.minor);
+    NMFB_CUDA_TRY(ctx, cudaSetDevice(device));
+    ctx->sm_count = prop.multiProcessorCount;
+    NMFB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+    ctx->stream = ctx->own_stream;
+    ctx->n = n;
+    ctx->m = m;
+    ctx->k = k;
+    ctx->kp = padded_rank(k);
+    ctx->ldv = ((size_t)m + 31) / 32 * 32;
+    size_t const kp = ctx->kp;
+    size_t const maxr = n > m ? n : m;
+    int rc;
+    if ((rc = dev_alloc(ctx, &ctx->dV, (size_t)n * ctx->ldv, "V"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dW, (size_t)n * kp, "W"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dH, (size_t)m * kp, "H"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dAccW, kp, "accW"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dAccH, kp, "accH"))) return rc;
+    // Split-reduction partials: the plans never exceed 2*SMs blocks of 64 outputs.
+    ctx->part_items = (size_t)NMFB_MAX_SPLIT * maxr * kp;
+    {
+        size_t const cap = (size_t)(2 * ctx->sm_count + 2) * 64 * kp + 2 * maxr * kp;
+        if (ctx->part_items > cap) ctx->part_items = cap;
+        if (ctx->part_items < 2 * maxr * kp) ctx->part_items = 2 * maxr * kp;
+    }
+    if ((rc = dev_alloc(ctx, &ctx->dPart, ctx->part_items, "partials"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dColPart, (size_t)2 * 1024 * kp, "colsum partials"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dTickets, 16, "tickets"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dObj, (size_t)3 * 1024 + 8, "objective"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dObjTicket, 4, "objective ticket"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dLabels, m, "labels"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dFirst, kp, "first"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dLastRep, m, "last rep"))) return rc;
+    if ((rc = dev_alloc(ctx, &ctx->dState, 1, "state"))) return rc;
+    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&ctx->hState, 2 * sizeof(ConvState)));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dTickets, 0, 16 * sizeof(uint32_t), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dObjTicket, 0, 4 * sizeof(uint32_t), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dV, 0, (size_t)n * ctx->ldv * sizeof(float), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dW, 0, (size_t)n * kp * sizeof(float), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dH, 0, (size_t)m * kp * sizeof(float), ctx->stream));
+    if ((rc = nmfb_reset_conv(ctx, 40))) return rc;
+    return nmfb_set_arm(ctx, arm);
+}
+
+int nmfb_set_arm(nmfb_ctx *ctx, int arm)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (arm != NMFB_ARM_FUSED && arm != NMFB_ARM_PLAIN && arm != NMFB_ARM_FUSED_TF32)
+        return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
+    ctx->arm = arm;
+    if (arm == NMFB_ARM_PLAIN) {
+        if (!ctx->dWH && (rc = dev_alloc(ctx, &ctx->dWH, (size_t)ctx->n * ctx->ldv, "WH"))) return rc;
+        return NMFB_OK;
+    }
+    if (!ctx->dWhi) {
+        size_t const kp = ctx->kp;
+        if ((rc = dev_alloc(ctx, &ctx->dWhi, (size_t)ctx->n * kp, "Whi"))) return rc;
+        if ((rc = dev_alloc(ctx, &ctx->dWlo, (size_t)ctx->n * kp, "Wlo"))) return rc;
+        if ((rc = dev_alloc(ctx, &ctx->dHhi, (size_t)ctx->m * kp, "Hhi"))) return rc;
+        if ((rc = dev_alloc(ctx, &ctx->dHlo, (size_t)ctx->m * kp, "Hlo"))) return rc;
+        if ((rc = refresh_splits(ctx))) return rc;
+    }
+    return nmfb_fused_prepare(ctx);
+}
+
+int nmfb_destroy(nmfb_ctx *ctx)
+{
+    if (!ctx) return NMFB_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+    return NMFB_OK;
+}
+
+const char *nmfb_last_error(const nmfb_ctx *ctx)
+{
+    if (!ctx) return "null context";
+    return ctx->err;
+}
+
+int nmfb_set_V(nmfb_ctx *ctx, const float *V, size_t ldv)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!V || ldv < ctx->m) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_V: null V or ldv (%zu) < m (%u)", ldv, ctx->m);
+    NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), V, ldv * sizeof(float),
+                                         ctx->m * sizeof(float), ctx->n, cudaMemcpyHostToDevice, ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->v_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_set_V_device(nmfb_ctx *ctx, const float *dV, size_t ldv)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!dV || ldv < ctx->m) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_V_device: null V or ldv < m");
+    NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), dV, ldv * sizeof(float),
+                                         ctx->m * sizeof(float), ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->v_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_init_random(nmfb_ctx *ctx, uint32_t seed)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    uint32_t const n = ctx->n, m = ctx->m, k = ctx->k;
+    float *W = (float *)malloc((size_t)n * k * sizeof(float));
+    float *H = (float *)malloc((size_t)m * k * sizeof(float));
+    if (!W || !H) {
+        free(W);
+        free(H);
+        return nmfb_fail(ctx, NMFB_ENOMEM, "host allocation for the initial factors");
+    }
+    // src/NMF_routines.c:206-233 and 299-307: srandom(seed); W first, then H;
+    // (float)random()/(float)RAND_MAX + FLT_MIN per factor entry.
+    srandom(seed);
+    for (size_t e = 0; e < (size_t)n * k; e++) W[e] = ((float)random()) / ((float)RAND_MAX) + FLT_MIN;
+    for (size_t e = 0; e < (size_t)m * k; e++) H[e] = ((float)random()) / ((float)RAND_MAX) + FLT_MIN;
+    rc = nmfb_set_WH(ctx, W, k, H, k);
+    free(W);
+    free(H);
+    return rc;
+}
+
+int nmfb_set_WH(nmfb_ctx *ctx, const float *W, size_t ldw, const float *H, size_t ldh)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!W || !H || ldw < ctx->k || ldh < ctx->k) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_WH: bad arguments");
+    if ((rc = upload_factor(ctx, ctx->dW, W, ctx->n, ctx->k, ldw))) return rc;
+    if ((rc = upload_factor(ctx, ctx->dH, H, ctx->m, ctx->k, ldh))) return rc;
+    if ((rc = refresh_splits(ctx))) return rc;
+    ctx->wh_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_update_H(nmfb_ctx *ctx)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    return do_update_H(ctx, 0);
+}
+
+int nmfb_update_W(nmfb_ctx *ctx)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    return do_update_W(ctx, 0);
+}
+
+int nmfb_adjust(nmfb_ctx *ctx)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    if ((rc = nmfb_adjust_rows(ctx, ctx->dH, ctx->m))) return rc;
+    return nmfb_adjust_rows(ctx, ctx->dW, ctx->n);
+}
+
+int nmfb_get_classification(nmfb_ctx *ctx, uint32_t *labels)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    if (!labels) return nmfb_fail(ctx, NMFB_EINVAL, "null labels");
+    if ((rc = nmfb_classify_only(ctx))) return rc;
+    NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(labels, ctx->dLabels, ctx->m * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return NMFB_OK;
+}
+
+int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold, uint32_t *iterations,
+             int *converged)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    if (n_iters == 0 || niter_test_conv == 0 || stop_threshold == 0)
+        return nmfb_fail(ctx, NMFB_EINVAL, "nIters, niter_test_conv and stop_threshold must be positive");
+    if ((rc = nmfb_reset_conv(ctx, stop_threshold))) return rc;
+    uint32_t const niter_conv = n_iters / niter_test_conv;
+    uint32_t const niter_rem = n_iters % niter_test_conv;
+    // Test blocks are queued in batches; the host looks at the device state of
+    // the previous batch (already finished or nearly so) before queueing more.
+    // Kernels queued after the stop rule fired return immediately.
+    uint32_t const batch = 4;
+    cudaEvent_t ev[2];
+    NMFB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    NMFB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    int stopped = 0;
+    uint32_t b = 0, q = 0;
+    while (b < niter_conv && !stopped) {
+        uint32_t const end = (b + batch < niter_conv) ? b + batch : niter_conv;
+        for (; b < end; b++) {
+            for (uint32_t i = 0; i < niter_test_conv && rc == 0; i++) {
+                rc = do_update_H(ctx, 0);
+                if (!rc) rc = do_update_W(ctx, i + 1 == niter_test_conv);
+            }
+            if (!rc) rc = nmfb_classify_and_test(ctx, niter_test_conv);
+            if (rc) break;
+        }
+        if (rc) break;
+        ConvState *slot = ctx->hState + (q & 1);
+        cudaError_t e = cudaMemcpyAsync(slot, ctx->dState, sizeof(ConvState), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[q & 1], ctx->stream);
+        if (e != cudaSuccess) {
+            rc = nmfb_fail(ctx, NMFB_ECUDA, "state copy: %s", cudaGetErrorString(e));
+            break;
+        }
+        if (q > 0) {
+            e = cudaEventSynchronize(ev[(q - 1) & 1]);
+            if (e != cudaSuccess) {
+                rc = nmfb_fail(ctx, NMFB_ECUDA, "event wait: %s", cudaGetErrorString(e));
+                break;
+            }
+            if (ctx->hState[(q - 1) & 1].converged) stopped = 1;
+        }
+        q++;
+    }
+    if (!rc && !stopped && niter_rem) {
+        // Remaining iterations without adjust; skipped on the device if converged.
+        for (uint32_t i = 0; i < niter_rem && rc == 0; i++) {
+            rc = do_update_H(ctx, 0);
+            if (!rc) rc = do_update_W(ctx, 0);
+        }
+    }
+    ConvState fin;
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(ctx->hState, ctx->dState, sizeof(ConvState), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = nmfb_fail(ctx, NMFB_ECUDA, "final state: %s", cudaGetErrorString(e));
+        fin = ctx->hState[0];
+        // Re-arm the kernels for single-step calls made after this run.
+        if (!rc) {
+            e = cudaMemsetAsync(&ctx->dState->converged, 0, sizeof(uint32_t), ctx->stream);
+            if (e != cudaSuccess) rc = nmfb_fail(ctx, NMFB_ECUDA, "re-arm: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (rc) return rc;
+    if (converged) *converged = fin.converged ? 1 : 0;
+    if (iterations) *iterations = fin.converged ? fin.conv_tests * niter_test_conv : n_iters;
+    return NMFB_OK;
+}
+
+int nmfb_get_W(nmfb_ctx *ctx, float *W, size_t ldw)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!W || ldw < ctx->k) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_get_W: bad arguments");
+    return download_factor(ctx, W, ctx->dW, ctx->n, ldw);
+}
+
+int nmfb_get_H(nmfb_ctx *ctx, float *H, size_t ldh)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!H || ldh < ctx->k) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_get_H: bad arguments");
+    return download_factor(ctx, H, ctx->dH, ctx->m, ldh);
+}
+
+int nmfb_dot_product_VWH(nmfb_ctx *ctx, double *dot_V, double *dot_VWH)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    return nmfb_objectives(ctx, dot_V, dot_VWH, nullptr);
+}
+
+int nmfb_kl_divergence(nmfb_ctx *ctx, double *kl)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    return nmfb_objectives(ctx, nullptr, nullptr, kl);
+}
+
+int nmfb_device_factors(nmfb_ctx *ctx, float **dW, float **dH, uint32_t *ldk)
+{
+    if (!ctx) return NMFB_EINVAL;
+    if (dW) *dW = ctx->dW;
+    if (dH) *dH = ctx->dH;
+    if (ldk) *ldk = ctx->kp;
+    return NMFB_OK;
+}
+
+int nmfb_device_V(nmfb_ctx *ctx, float **dV, size_t *ldv)
+{
+    if (!ctx) return NMFB_EINVAL;
+    if (dV) *dV = ctx->dV;
+    if (ldv) *ldv = ctx->ldv;
+    return NMFB_OK;
+}
+
+int nmfb_set_stream(nmfb_ctx *ctx, void *stream)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return NMFB_OK;
+}
+
+static int prof_harvest(nmfb_ctx *ctx, int cls)
+{
+    uint32_t const n = ctx->prof_n[cls];
+    if (n == 0) return NMFB_OK;
+    cudaEvent_t *ev = ctx->prof_ev[cls];
+    NMFB_CUDA_TRY(ctx, cudaEventSynchronize(ev[2 * n - 1]));
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; i++) {
+        float ms = 0.0f;
+        NMFB_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
+        s += ms;
+    }
+    ctx->prof_ms[cls] += s;
+    ctx->prof_cnt[cls] += n;
+    ctx->prof_n[cls] = 0;
+    return NMFB_OK;
+}
+
+int nmfb_prof_begin(nmfb_ctx *ctx, int cls)
+{
+    if (!ctx->prof_on) return NMFB_OK;
+    if (ctx->prof_n[cls] == NMFB_PROF_POOL) {
+        int rc = prof_harvest(ctx, cls);
+        if (rc) return rc;
+    }
+    NMFB_CUDA_TRY(ctx, cudaEventRecord(ctx->prof_ev[cls][2 * ctx->prof_n[cls]], ctx->stream));
+    return NMFB_OK;
+}
+
+int nmfb_prof_end(nmfb_ctx *ctx, int cls)
+{
+    if (!ctx->prof_on) return NMFB_OK;
+    NMFB_CUDA_TRY(ctx, cudaEventRecord(ctx->prof_ev[cls][2 * ctx->prof_n[cls] + 1], ctx->stream));
+    ctx->prof_n[cls]++;
+    return NMFB_OK;
+}
+
+int nmfb_profile(nmfb_ctx *ctx, int enable)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    for (int c = 0; c < 4; c++) {
+        if (enable && !ctx->prof_ev[c]) {
+            ctx->prof_ev[c] = (cudaEvent_t *)calloc(2 * NMFB_PROF_POOL, sizeof(cudaEvent_t));
+            if (!ctx->prof_ev[c]) return nmfb_fail(ctx, NMFB_ENOMEM, "profile events");
+            for (int i = 0; i < 2 * NMFB_PROF_POOL; i++)
+                NMFB_CUDA_TRY(ctx, cudaEventCreate(&ctx->prof_ev[c][i]));
+        }
+        ctx->prof_n[c] = 0;
+        ctx->prof_ms[c] = 0.0;
+        ctx->prof_cnt[c] = 0;
+    }
+    ctx->prof_on = enable ? 1 : 0;
+    return NMFB_OK;
+}
+
+int nmfb_profile_read(nmfb_ctx *ctx, int cls, double *total_ms, uint32_t *count)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (cls < 0 || cls > 3) return nmfb_fail(ctx, NMFB_EINVAL, "profile class %d", cls);
+    if (ctx->prof_ev[cls] && (rc = prof_harvest(ctx, cls))) return rc;
+    if (total_ms) *total_ms = ctx->prof_ms[cls];
+    if (count) *count = ctx->prof_cnt[cls];
+    return NMFB_OK;
+}
+
+int nmfb_synchronize(nmfb_ctx *ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return NMFB_OK;
+}
+
+uint64_t nmfb_launch_count(const nmfb_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// nmfb_internal.cuh -- engine-private declarations shared by the .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/nmfb200.h"
+
+namespace nmfb {
+
+// Device-side state of the convergence test (src/NMF_GPU.c:544-709).
+struct ConvState {
+    uint32_t inc;          // tests without change (reference `inc`)
+    uint32_t converged;    // 1 once the stop rule fired; later kernels are no-ops
+    uint32_t tests_done;   // convergence tests performed
+    uint32_t conv_tests;   // value of `iter` (tests counted) at convergence
+    uint32_t diff;         // any connectivity difference found by the current test
+    uint32_t ticket;       // block retirement counter of the compare kernel
+    uint32_t stop_threshold;
+    uint32_t pad;
+};
+
+// Scratch for one deterministic column-sum reduction.
+struct ColsumScratch {
+    double *part;        // [blocks][kp]
+    uint32_t *ticket;
+};
+
+}  // namespace nmfb
+
+struct nmfb_ctx {
+    int device;
+    int arm;
+    cudaStream_t stream;
+    uint32_t n, m, k, kp;  // kp: internal padded rank (16, 32, or a multiple of 32)
+    size_t ldv;            // leading dimension of V on the device (items, multiple of 32)
+    int v_set, wh_set;
+
+    float *dV;             // n x ldv
+    float *dW, *dH;        // n x kp, m x kp (padding columns zero)
+    float *dAccW, *dAccH;  // kp each: column sums of W and of H
+    float *dWH;            // plain arm: n x ldv quotient buffer
+    float *dPart;          // split-reduction partials (max(n, m) x kp x nsplit)
+    size_t part_items;
+    double *dColPart;      // colsum partials
+    uint32_t *dTickets;    // [0]: colsum W, [1]: colsum H, [2..]: misc
+    double *dObj;          // objective partials + results
+    uint32_t *dObjTicket;
+
+    // tcgen05 arm: hi/lo tf32 splits of the factors (row-major, kp columns).
+    float *dWhi, *dWlo, *dHhi, *dHlo;
+    int sm_count;
+    void *tmaps;           // fused-arm tensor maps (host copy), see kernels_fused.cu
+
+    // Convergence test state.
+    uint32_t *dLabels;     // m
+    uint32_t *dFirst;      // kp: first sample index of every label
+    uint32_t *dLastRep;    // m: canonical partition of the previous test
+    nmfb::ConvState *dState;
+    nmfb::ConvState *hState;  // pinned host mirror
+
+    uint64_t launches;
+    cudaStream_t own_stream;
+
+    // Event profiling (nmfb_profile): per class a pool of (start, stop) pairs.
+    int prof_on;
+    cudaEvent_t *prof_ev[4];
+    uint32_t prof_n[4];
+    double prof_ms[4];
+    uint32_t prof_cnt[4];
+    char err[512];
+};
+
+// ---- error helpers -------------------------------------------------------
+int nmfb_fail(nmfb_ctx *ctx, int code, const char *fmt, ...);
+
+#define NMFB_CUDA_TRY(ctx, call)                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return nmfb_fail((ctx), NMFB_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                             __FILE__, __LINE__);                                            \
+    } while (0)
+
+#define NMFB_LAUNCH_CHECK(ctx)                                                               \
+    do {                                                                                     \
+        (ctx)->launches++;                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                                 \
+        if (e_ != cudaSuccess)                                                               \
+            return nmfb_fail((ctx), NMFB_ECUDA, "kernel launch: %s (%s:%d)",                 \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+    } while (0)
+
+// ---- profiling (nmfb_api.cu) ---------------------------------------------------
+#define NMFB_PROF_POOL 512
+extern "C" int nmfb_prof_begin(nmfb_ctx *ctx, int cls);
+extern "C" int nmfb_prof_end(nmfb_ctx *ctx, int cls);
+
+// ---- kernels_common.cu ----------------------------------------------------
+int nmfb_colsum(nmfb_ctx *ctx, const float *X, uint32_t rows, float *acc, int which);
+int nmfb_muldiv(nmfb_ctx *ctx, float *X, uint32_t rows, const float *part, uint32_t nsplit,
+                size_t split_stride, const float *acc, int adjust, float *hi, float *lo);
+int nmfb_adjust_rows(nmfb_ctx *ctx, float *X, uint32_t rows);
+int nmfb_classify_and_test(nmfb_ctx *ctx, uint32_t niter_test_conv);
+int nmfb_classify_only(nmfb_ctx *ctx);
+int nmfb_reset_conv(nmfb_ctx *ctx, uint32_t stop_threshold);
+int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl);
+int nmfb_split_tf32(nmfb_ctx *ctx, const float *X, uint32_t rows, float *hi, float *lo);
+
+// ---- kernels_plain.cu -----------------------------------------------------
+int nmfb_plain_update_H(nmfb_ctx *ctx, int adjust);
+int nmfb_plain_update_W(nmfb_ctx *ctx, int adjust);
+
+// ---- kernels_fused.cu -----------------------------------------------------
+int nmfb_fused_prepare(nmfb_ctx *ctx);
+int nmfb_fused_release(nmfb_ctx *ctx);
+int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust);
+int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust);
+
+// Max number of reduction splits used by any arm (sizes dPart).
+#define NMFB_MAX_SPLIT 64

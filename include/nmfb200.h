@@ -1,0 +1,165 @@
+/*
+ * nmfb200.h -- C ABI of the B200-native KL-NMF engine (drop-in for the
+ * single-GPU path of NMF-mGPU / bioinfo-cnb/bionmf-gpu).
+ *
+ * The reference keeps all device state in globals (src/GPU_setup.c:191-285)
+ * and exposes its loop through the entry points cited below.  This library
+ * holds that state in an opaque context instead; one context = one
+ * factorisation V (n x m) ~ W (n x k) * H (k x m) on one device.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, integers.  No CUDA or torch types.
+ *  - Host matrices are row-major with an explicit leading dimension in items.
+ *    H is exchanged as the reference stores it, "transposed": m rows of k
+ *    factors (src/NMF_GPU.c:70-76), unless a function says otherwise.
+ *  - Every function returns 0 (NMFB_OK) on success or a negative NMFB_E* code;
+ *    nmfb_last_error() describes the last failure of a context.  There is no
+ *    CPU fallback: without a usable sm_100 device nmfb_create() fails.
+ *  - A context is not thread-safe; use one host thread per context.
+ *  - Work is queued on the context's CUDA stream; functions that return host
+ *    data synchronise that stream.
+ */
+#ifndef NMFB200_H
+#define NMFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NMFB_OK 0
+#define NMFB_EINVAL (-1)   /* invalid argument (sizes, rank, null pointer) */
+#define NMFB_ECUDA (-2)    /* CUDA runtime error (message in nmfb_last_error) */
+#define NMFB_ENOMEM (-3)   /* device or pinned memory allocation failed */
+#define NMFB_ENODEV (-4)   /* no sm_100 device / extension not usable */
+#define NMFB_ESTATE (-5)   /* call out of order (e.g. update before V is set) */
+#define NMFB_ETIMEOUT (-6) /* a bounded device wait ran out */
+
+/* Update kernels ("arms").  All arms run the same method; they differ only
+ * in how the two n x m x k contractions of a half-iteration are evaluated. */
+#define NMFB_ARM_FUSED 0  /* fused half-iteration, tcgen05 3xTF32 (FP32-accurate) */
+#define NMFB_ARM_PLAIN 1  /* unfused FP32 SIMT kernels mirroring the reference's 5 steps */
+#define NMFB_ARM_FUSED_TF32 2 /* fused, 1xTF32 denominator (reduced precision) */
+
+typedef struct nmfb_ctx nmfb_ctx;
+
+/* Library version string. */
+const char *nmfb_version(void);
+
+/* Number of CUDA devices usable by the engine (sm_100 class); 0 if none. */
+int nmfb_device_count(void);
+
+/*
+ * initialize_GPU + setup_GPU (src/GPU_setup.c:569-868, 2105-2239).
+ * Creates a context for an n x m input and rank k on `device`, allocating all
+ * device buffers.  Fails with NMFB_EINVAL if k < 2, k > min(n, m) (as
+ * src/NMF_GPU.c:1121-1128) or k > 256, and with NMFB_ENOMEM if the matrices
+ * do not fit the device.
+ */
+int nmfb_create(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uint32_t k, int arm);
+
+/* finalize_GPU_device (src/GPU_setup.c:2291): frees everything. NULL is a no-op. */
+int nmfb_destroy(nmfb_ctx *ctx);
+
+/* Last error message of this context (never NULL). */
+const char *nmfb_last_error(const nmfb_ctx *ctx);
+
+/* Select the update arm (NMFB_ARM_*) of an existing context. */
+int nmfb_set_arm(nmfb_ctx *ctx, int arm);
+
+/*
+ * init_V's upload (src/NMF_GPU.c:212-303 + upload_matrix_partial,
+ * src/matrix_operations.c:1712-1905): copies V (n x m, host, row-major,
+ * leading dimension ldv >= m) to the device.  Values must be finite and >= 0.
+ */
+int nmfb_set_V(nmfb_ctx *ctx, const float *V, size_t ldv);
+
+/* Same, from a device pointer (device-to-device copy on the context stream). */
+int nmfb_set_V_device(nmfb_ctx *ctx, const float *dV, size_t ldv);
+
+/*
+ * init_random + set_random_values in the reference's CPU_RANDOM mode
+ * (src/NMF_routines.c:206-233, 271-362): srandom(seed), then W row by row and
+ * H row by row, each value (float)random()/(float)RAND_MAX + FLT_MIN.
+ * Bit-identical to the reference's host initialisation for the same seed.
+ */
+int nmfb_init_random(nmfb_ctx *ctx, uint32_t seed);
+
+/* Upload explicit initial factors: W (n x k, ldw >= k), H (m x k, ldh >= k). */
+int nmfb_set_WH(nmfb_ctx *ctx, const float *W, size_t ldw, const float *H, size_t ldh);
+
+/* update_H (src/NMF_routines.c:704-1000): H = H .* (W' (V ./ (W H))) ./ colsum(W). */
+int nmfb_update_H(nmfb_ctx *ctx);
+
+/* update_W (src/NMF_routines.c:1344-1636): W = W .* ((V ./ (W H)) H') ./ colsum(H). */
+int nmfb_update_W(nmfb_ctx *ctx);
+
+/* matrix_adjust on H then W (src/NMF_GPU.c:611-638; src/GPU_kernels.cu:2220-2370). */
+int nmfb_adjust(nmfb_ctx *ctx);
+
+/*
+ * get_classification (src/NMF_routines.c:1646-1744): for each of the m
+ * samples, the index of its largest factor in H, with the reference's tie
+ * rule (kernel_idx_max, src/GPU_kernels.cu:3177-3267).  `labels` is a host
+ * array of m entries.  Synchronises the stream.
+ */
+int nmfb_get_classification(nmfb_ctx *ctx, uint32_t *labels);
+
+/*
+ * nmf() (src/NMF_GPU.c:312-924, loop :522-795): runs up to n_iters
+ * iterations, testing convergence every niter_test_conv iterations (adjust H
+ * and W, classify, compare connectivity with the previous test) and stopping
+ * once the classification has not changed for stop_threshold more tests.
+ * The stable-count and stop flag live on the device; the host does not read
+ * them after every test.  Outputs the iterations performed (iter * J on
+ * convergence, else n_iters) and whether it converged.
+ */
+int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold,
+             uint32_t *iterations, int *converged);
+
+/* Download W (n x k into ldw >= k) and H (m x k into ldh >= k). */
+int nmfb_get_W(nmfb_ctx *ctx, float *W, size_t ldw);
+int nmfb_get_H(nmfb_ctx *ctx, float *H, size_t ldh);
+
+/*
+ * dot_product_VWH (src/NMF_routines.c:2680-2794), FP64 accumulation:
+ * dot_V = ||V||^2, dot_VWH = ||V - W H||^2.  The reference prints
+ * sqrt(dot_VWH)/sqrt(dot_V) as "Distance between V and W*H".
+ */
+int nmfb_dot_product_VWH(nmfb_ctx *ctx, double *dot_V, double *dot_VWH);
+
+/* Generalised KL divergence sum(V log(V/WH) - V + WH) in FP64 (0 log 0 = 0).
+ * The reference has no counterpart; it is the objective the updates descend. */
+int nmfb_kl_divergence(nmfb_ctx *ctx, double *kl);
+
+/* Raw device pointers of the factors (for zero-copy callers): W is n x ldk,
+ * H is m x ldk, row-major, float, padding columns zero. */
+int nmfb_device_factors(nmfb_ctx *ctx, float **dW, float **dH, uint32_t *ldk);
+
+/* Device pointer and leading dimension of V inside the context. */
+int nmfb_device_V(nmfb_ctx *ctx, float **dV, size_t *ldv);
+
+/* Queue the context's work on `stream` (a cudaStream_t passed as void*; NULL
+ * restores the context's own stream).  The caller keeps ownership. */
+int nmfb_set_stream(nmfb_ctx *ctx, void *stream);
+
+/* Device-time profiling of the update kernels with CUDA events recorded on the
+ * context stream around each launch.  enable=1 starts (and clears) the record;
+ * nmfb_profile_read() synchronises and returns, for kernel class `cls`
+ * (0: update_H main kernel, 1: update_W main kernel, 2: whole update_H,
+ * 3: whole update_W), the summed milliseconds and the number of launches. */
+int nmfb_profile(nmfb_ctx *ctx, int enable);
+int nmfb_profile_read(nmfb_ctx *ctx, int cls, double *total_ms, uint32_t *count);
+
+/* Block the host until all queued work of the context is done. */
+int nmfb_synchronize(nmfb_ctx *ctx);
+
+/* Kernel launches issued by this context since creation (for accounting). */
+uint64_t nmfb_launch_count(const nmfb_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NMFB200_H */

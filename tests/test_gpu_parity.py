@@ -1,0 +1,153 @@
+"""GPU parity tests: the CUDA engine (through the C ABI) against the CPU oracle
+and against fixtures produced by the reference's own CUDA build.
+
+Tolerances (stated per the north star):
+  * W, H after a fixed iteration count: max|dX| / max|X| <= 1e-4 against the
+    FP32 oracle and the FP64 oracle;
+  * runs to convergence: identical iteration count and classification; W, H
+    within 2e-3 (FP32 drift over hundreds of iterations, measured between the
+    FP32 and FP64 oracles, is of that order);
+  * KL divergence: 1e-5 relative against the FP64 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, maxnorm_rel
+
+pytestmark = pytest.mark.gpu
+
+ARMS = ["plain", "fused"]
+
+
+def _engine(pkg, V, k, arm, seed=3):
+    e = pkg.NMF(V.shape[0], V.shape[1], k, arm=arm)
+    e.set_V(V)
+    e.init_random(seed)
+    return e
+
+
+@pytest.mark.parametrize("arm", ARMS)
+@pytest.mark.parametrize("shape", [(37, 19, 2), (300, 70, 5), (1000, 130, 16), (700, 333, 33), (257, 190, 64)])
+def test_single_half_updates(pkg, oracle, synth, arm, shape):
+    n, m, k = shape
+    V, _ = synth.expression_like(n, m, k, seed=n + m)
+    W0, H0 = oracle.init_random(3, n, m, k)
+    with _engine(pkg, V, k, arm) as e:
+        assert np.array_equal(e.W, W0) and np.array_equal(e.H, H0)
+        e.update_H()
+        H1 = oracle.update_H(V, W0, H0, prec="f64")
+        assert maxnorm_rel(e.H, H1) < 1e-5
+        e.update_W()
+        W1 = oracle.update_W(V, W0, H1, prec="f64")
+        assert maxnorm_rel(e.W, W1) < 1e-5
+
+
+@pytest.mark.parametrize("arm", ARMS)
+def test_fixed_iterations_config_a(pkg, oracle, synth, arm):
+    V, _ = synth.config_a(1)
+    n, m = V.shape
+    W0, H0 = oracle.init_random(3, n, m, 3)
+    W64, H64, _, _ = oracle.nmf(V, W0, H0, 50, 100, 40, prec="f64")
+    W32, H32, _, _ = oracle.nmf(V, W0, H0, 50, 100, 40, prec="f32")
+    with _engine(pkg, V, 3, arm) as e:
+        it, conv = e.run(50, 100, 40)
+        assert (it, conv) == (50, False)
+        for ref in ((W64, H64), (W32, H32)):
+            assert maxnorm_rel(e.W, ref[0]) < 1e-4
+            assert maxnorm_rel(e.H, ref[1]) < 1e-4
+
+
+@pytest.mark.parametrize("arm", ARMS)
+def test_convergence_loop_matches_oracle(pkg, oracle, synth, arm):
+    V, _ = synth.config_d(4)
+    n, m = V.shape
+    W0, H0 = oracle.init_random(3, n, m, 5)
+    Wr, Hr, it_r, conv_r = oracle.nmf(V, W0, H0, 2000, 10, 40)
+    with _engine(pkg, V, 5, arm) as e:
+        it, conv = e.run(2000, 10, 40)
+        assert (it, conv) == (it_r, conv_r)
+        assert np.array_equal(e.classification(), oracle.classify(Hr))
+        assert maxnorm_rel(e.W, Wr) < 2e-3 and maxnorm_rel(e.H, Hr) < 2e-3
+
+
+@pytest.mark.parametrize("arm", ARMS)
+def test_kl_divergence_vs_fp64(pkg, oracle, synth, arm):
+    V, _ = synth.expression_like(3000, 400, 8, seed=21, zero_frac=0.01)
+    n, m = V.shape
+    W0, H0 = oracle.init_random(3, n, m, 8)
+    W64, H64, _, _ = oracle.nmf(V, W0, H0, 30, 10, 1000, prec="f64")
+    kl64 = oracle.kl_divergence(V, W64.astype(np.float32), H64.astype(np.float32))
+    with _engine(pkg, V, 8, arm) as e:
+        e.run(30, 10, 1000)
+        kl = e.kl_divergence()
+        # the FP64 objective of the engine's own factors equals the oracle's on them
+        assert abs(kl - oracle.kl_divergence(V, e.W, e.H)) <= 1e-9 * abs(kl)
+        assert abs(kl - kl64) <= 1e-5 * abs(kl64)
+        a, b = e.dot_product_VWH()
+        ra, rb = oracle.dot_VWH(V, e.W, e.H)
+        assert abs(a - ra) <= 1e-9 * ra and abs(b - rb) <= 1e-7 * rb
+
+
+@pytest.mark.parametrize("arm", ARMS)
+def test_classification_entry_point(pkg, oracle, synth, arm):
+    V, labels = synth.expression_like(2000, 150, 6, seed=5)
+    with _engine(pkg, V, 6, arm) as e:
+        e.run(200, 10, 1000)
+        H = e.H
+        assert np.array_equal(e.classification(), oracle.classify(H))
+
+
+def test_ties_on_device(pkg, oracle):
+    # Exact ties in H must resolve as the reference's warp reduction does.
+    n, m, k = 64, 40, 32
+    V = np.ones((n, m), np.float32)
+    H = np.zeros((m, k), np.float32)
+    H[:, 5] = 1.0
+    H[1, 8] = H[1, 16] = 2.0
+    H[2, :] = 1.0
+    H[3, 3] = H[3, 1] = 7.0
+    W = np.ones((n, k), np.float32)
+    with pkg.NMF(n, m, k, arm="plain") as e:
+        e.set_V(V)
+        e.set_WH(W, H)
+        assert np.array_equal(e.classification(), oracle.classify(H))
+
+
+@pytest.mark.parametrize("arm", ARMS)
+def test_zero_entries_and_ragged_sizes(pkg, oracle, synth, arm):
+    V, _ = synth.expression_like(1111, 97, 7, seed=8, zero_frac=0.05)
+    W0, H0 = oracle.init_random(3, 1111, 97, 7)
+    Wr, Hr, _, _ = oracle.nmf(V, W0, H0, 20, 10, 1000, prec="f64")
+    with _engine(pkg, V, 7, arm) as e:
+        e.run(20, 10, 1000)
+        assert maxnorm_rel(e.W, Wr) < 1e-4 and maxnorm_rel(e.H, Hr) < 1e-4
+
+
+def test_invalid_arguments(pkg):
+    with pytest.raises(pkg.NMFError):
+        pkg.NMF(100, 10, 11)
+    with pkg.NMF(100, 10, 3) as e:
+        with pytest.raises(pkg.NMFError) as ei:
+            e.update_H()          # V not set yet
+        assert ei.value.code == -5
+
+
+CASES = golden_cases()
+
+
+@pytest.mark.skipif(not CASES, reason="no reference fixtures")
+@pytest.mark.parametrize("arm", ARMS)
+@pytest.mark.parametrize("case", CASES)
+def test_engine_matches_reference_fixture(pkg, oracle, case, arm):
+    g = load_golden(case)
+    V = g["V"]
+    k = int(g["k"])
+    with _engine(pkg, V, k, arm, seed=int(g["seed"])) as e:
+        it, conv = e.run(int(g["n_iters"]), int(g["niter_test_conv"]), int(g["stop_threshold"]))
+        assert it == int(g["iterations"]) and conv == bool(g["converged"])
+        tol = 1e-4 if int(g["n_iters"]) <= 100 else 2e-3
+        assert maxnorm_rel(e.W, g["W"]) < tol and maxnorm_rel(e.H, g["H"]) < tol
+        assert np.array_equal(e.classification(), oracle.classify(g["H"]))
+        assert abs(e.distance() - float(g["distance"])) <= 1e-5 * float(g["distance"]) + 5e-7
