@@ -60,7 +60,20 @@ def golden_cases():
 
 
 def load_golden(name):
-    return dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
+    """Load a reference-run fixture; regenerate V from its seeded generator
+    when the fixture stores only the generator call and V's SHA-256."""
+    import hashlib
+    import json
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
+    if "V" not in g:
+        load_package()
+        import nmf_b200.synth as synth
+        gen, kw = json.loads(str(g["generator"]))
+        V, _ = getattr(synth, gen)(**kw)
+        assert hashlib.sha256(np.ascontiguousarray(V, np.float32).tobytes()).hexdigest() == str(g["v_sha256"]), \
+            f"{name}: regenerated V does not match the fixture's hash"
+        g["V"] = V
+    return g
 
 
 def maxnorm_rel(a, b):

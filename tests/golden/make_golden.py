@@ -8,13 +8,15 @@ outputs (``-e 0``: little-endian float64) and its stdout.  Needs a GPU.
 
     python tests/golden/make_golden.py --out gpurun_out/golden
 
-Each case is written as ``<case>.npz`` holding the input V (float32), the
+Each case is written as ``<case>.npz`` holding the input V (float32; for
+inputs above 200k entries only the generator call and the SHA-256 of V), the
 reference's W (n x k) and H (m x k, un-transposed), the iteration count, the
 "converged" flag, the printed Frobenius distance and the arguments used.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import importlib.util
 import json
 import os
@@ -75,11 +77,24 @@ def make_input(synth, gen):
     return V, labels
 
 
+def safe_input_path(tmp, name):
+    """The reference allocates strlen(filename) + strlen(ext) bytes for the
+    output name "<filename>_W<ext>" (src/NMF_GPU.c:975-990), three bytes short.
+    Pick a path length whose malloc rounding leaves room for those bytes."""
+    base = os.path.join(tmp, name)
+    while True:
+        s = len(base) + 4                      # what the reference passes to malloc
+        chunk = max(32, (s + 8 + 15) & ~15)    # glibc chunk size
+        if chunk - 8 >= s + 3:
+            return base
+        base += "_"
+
+
 def run_case(name, spec, outdir, tmp):
     synth = _synth()
     (gen, k, it, j, t) = spec
     V, labels = make_input(synth, gen)
-    fn = os.path.join(tmp, name)
+    fn = safe_input_path(tmp, name)
     write_binary(fn, V)
     cmd = [REF_BIN, fn, "-b", "0", "-e", "0", "-k", str(k), "-i", str(it), "-j", str(j), "-t", str(t)]
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
@@ -93,10 +108,13 @@ def run_case(name, spec, outdir, tmp):
     iters = int(m_conv.group(1)) if m_conv else int(m_perf.group(1))
     dist = float(re.search(r"Distance between V and W\*H: ([0-9.eE+-]+)", out).group(1))
     gpu_t = re.search(r"GPU \+ classification \+ check_result time: ([0-9.eE+-]+)", out)
-    np.savez_compressed(os.path.join(outdir, name + ".npz"), V=V, labels=labels, W=W.astype(np.float32),
-                        H=np.ascontiguousarray(Ht.T).astype(np.float32), iterations=iters,
-                        converged=bool(m_conv), distance=dist, k=k, n_iters=it, niter_test_conv=j,
-                        stop_threshold=t, seed=3, stdout=out)
+    fields = dict(labels=labels, W=W.astype(np.float32), H=np.ascontiguousarray(Ht.T).astype(np.float32),
+                  iterations=iters, converged=bool(m_conv), distance=dist, k=k, n_iters=it, niter_test_conv=j,
+                  stop_threshold=t, seed=3, stdout=out, generator=json.dumps([gen[0], gen[1]]),
+                  v_sha256=hashlib.sha256(np.ascontiguousarray(V, np.float32).tobytes()).hexdigest())
+    if V.size <= 200000:   # larger inputs are regenerated from the seeded generator
+        fields["V"] = V
+    np.savez_compressed(os.path.join(outdir, name + ".npz"), **fields)
     return dict(case=name, iterations=iters, converged=bool(m_conv), distance=dist,
                 gpu_seconds=float(gpu_t.group(1)) if gpu_t else None)
 
