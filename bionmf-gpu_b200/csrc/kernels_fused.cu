@@ -1,7 +1,811 @@
-// kernels_fused.cu -- fused half-iteration arm (placeholder until the tcgen05 kernel lands).
+// kernels_fused.cu -- the fused half-iteration arm (NMFB_ARM_FUSED / _FUSED_TF32).
+//
+// One kernel computes, for a block of 128 rows of the factor being updated
+// (X = W for update_W, X = H for update_H) and a range of the reduction
+// dimension, the partial  Xaux = sum_r  (V ./ (X Y^T))[o][r] * Y[r][:]
+// without ever materialising the n x m quotient:
+//
+//   TMA      : V tile (128 x BR, FP32), Y tile (BR x KP) and its transpose
+//              Y^T tile (KP x BR), each as TF32 hi and lo parts, into a
+//              STAGES-deep shared-memory ring; X (128 x KP, hi/lo) once.
+//   MMA1     : D (TMEM, 128 x BR, FP32) = Xh Yh^T + Xh Yl^T + Xl Yh^T
+//              (tcgen05.mma kind::tf32, A and B from shared memory, K-major).
+//   epilogue : R = V / D in FP32 registers (fdividef, as the reference),
+//              split R = Rh + Rl (Rh = TF32 round-to-nearest), written back to TMEM.
+//   MMA2     : Acc (TMEM, 128 x KP) += Rh Yh + Rh Yl + Rl Yh
+//              (kind::tf32, A = R from TMEM, B = the Y^T tile, K-major; an
+//              MN-major read of the Y tile returns zeros for TF32 on sm_100a,
+//              so the transposed copy of each factor is kept in HBM).
+//   end      : Acc -> the split's partial in global memory; k_muldiv (kernels_common.cu)
+//              sums the splits and applies X = X .* Xaux ./ colsum(Y).
+//
+// Reference equivalent: get_H_BLM / get_W_BLN (src/NMF_routines.c:376-525,
+// 1014-1164): two cuBLAS SGEMMs around matrix_div_sub with WH in HBM.
+//
+// Warp roles (384 threads): warp 0 = V producer (TMA), warp 1 = MMA issuer and
+// TMEM owner, warp 2 = X/Y producer (TMA), warps 4-11 = epilogue (warp w
+// reads TMEM lanes 32*(w%4)..+31, column half (w-4)/4 of every tile).  V
+// stages are released as soon as the epilogue has read them; Y stages when
+// the second MMA that reads them has completed.
+// Every mbarrier wait is bounded (1 s of %globaltimer); on expiry the kernel
+// records an error word that the host turns into NMFB_ETIMEOUT.
+// No TMA multicast is used anywhere.
 #include "nmfb_internal.cuh"
 
-int nmfb_fused_prepare(nmfb_ctx *ctx) { (void)ctx; return NMFB_OK; }
-int nmfb_fused_release(nmfb_ctx *ctx) { (void)ctx; return NMFB_OK; }
-int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust) { (void)adjust; return nmfb_fail(ctx, NMFB_ENODEV, "fused arm not built"); }
-int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust) { (void)adjust; return nmfb_fail(ctx, NMFB_ENODEV, "fused arm not built"); }
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+using nmfb::ConvState;
+
+namespace {
+
+constexpr int BO = 128;          // output rows per CTA = TMEM lanes
+constexpr int NTHREADS = 384;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr int SMEM_LIMIT = 232448; // max dynamic shared memory per block on sm_100
+constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;
+
+struct FusedMaps {
+    CUtensorMap v;
+    CUtensorMap xh, xl;  // updated factor, box rows = BO
+    CUtensorMap yh, yl;  // other factor, box rows = BR
+    CUtensorMap yth, ytl;  // other factor transposed (KP x rows), box = 32 x KP
+};
+
+struct FusedArgs {
+    uint32_t O, R;        // output rows, reduction length
+    uint32_t tiles_per_split, nsplit;
+    float *part;          // [split][O][KP]
+    uint32_t *err;        // device error word
+    const ConvState *st;
+#ifdef NMFB_FUSED_DEBUG
+    float *dbg;           // block 0, tile 0: D | V | Rh | Acc (debug builds only; 128 x 64 each)
+#endif
+};
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false on timeout or when another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort_flag,
+                                          uint32_t *err, uint32_t code)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    unsigned long long const t0 = globaltimer();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort_flag) return false;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            *abort_flag = 1;
+            atomicExch(err, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+#define NMFB_R32(a) \
+    "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]), "=r"(a[8]), \
+        "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]), "=r"(a[15]), "=r"(a[16]), \
+        "=r"(a[17]), "=r"(a[18]), "=r"(a[19]), "=r"(a[20]), "=r"(a[21]), "=r"(a[22]), "=r"(a[23]), "=r"(a[24]), \
+        "=r"(a[25]), "=r"(a[26]), "=r"(a[27]), "=r"(a[28]), "=r"(a[29]), "=r"(a[30]), "=r"(a[31])
+#define NMFB_W32(a) \
+    "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(a[8]), "r"(a[9]), \
+        "r"(a[10]), "r"(a[11]), "r"(a[12]), "r"(a[13]), "r"(a[14]), "r"(a[15]), "r"(a[16]), "r"(a[17]), "r"(a[18]), \
+        "r"(a[19]), "r"(a[20]), "r"(a[21]), "r"(a[22]), "r"(a[23]), "r"(a[24]), "r"(a[25]), "r"(a[26]), "r"(a[27]), \
+        "r"(a[28]), "r"(a[29]), "r"(a[30]), "r"(a[31])
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : NMFB_R32(r)
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        NMFB_W32(r)
+        : "memory");
+}
+
+// tcgen05.wait::ld that also ties the loaded registers to the wait, so that no use of
+// them can be scheduled before the load has completed.
+__device__ __forceinline__ void tmem_wait_ld_dep(uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.wait::ld.sync.aligned;"
+        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+          "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]),
+          "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+          "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+        :
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Shared-memory matrix descriptor (tcgen05): start address, leading / stride
+// byte offsets (16-byte units), version 1, swizzle layout in bits 61-63.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout)
+{
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)layout << 61;
+    return d;
+}
+
+// Instruction descriptor for kind::tf32 with FP32 accumulation, A K-major.
+__host__ __device__ constexpr uint32_t idesc_tf32(uint32_t M, uint32_t N, uint32_t b_mn_major)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | (b_mn_major << 16) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------
+template <int KP>
+struct Geo {
+    static constexpr int BR = (KP >= 64) ? 32 : 64;       // reduction rows per tile
+    static constexpr int CB = (KP == 16) ? 16 : 32;       // floats per swizzle column block
+    static constexpr int NB = KP / CB;                     // column blocks
+    static constexpr int ROWB = CB * 4;                    // bytes per row of a block
+    static constexpr uint32_t LAYOUT = (KP == 16) ? 4u : 2u;  // SW64 : SW128
+    static constexpr int XBLK = BO * ROWB;                 // bytes of one X column block
+    static constexpr int YBLK = BR * ROWB;                 // bytes of one Y column block
+    static constexpr int YTBLK = KP * 128;                 // bytes of one Y^T block (32 reduction rows)
+    static constexpr int XBYTES = BO * KP * 4;
+    static constexpr int YBYTES = BR * KP * 4;
+    static constexpr int VBYTES = BO * BR * 4;
+    static constexpr int YSTAGE = 4 * YBYTES;              // Yh | Yl | YTh | YTl
+    static constexpr int YST = 3;                          // Y ring depth (L2-resident operand)
+    static constexpr int FIXED = 1024 + 2 * XBYTES + 512;
+    static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YST * YSTAGE) / VBYTES;
+    static constexpr int VST = VAVAIL > 6 ? 6 : VAVAIL;    // V ring depth (HBM stream)
+    static constexpr int SMEM = FIXED + YST * YSTAGE + VST * VBYTES;
+    static constexpr int HALF = KP / 2;                    // accumulator columns per epilogue warp
+    static_assert(VST >= 2, "shared-memory ring too small");
+};
+
+// TMEM columns: per-tile accumulators Acc[b] at b*64 (KP <= 64 columns each),
+// D[b] (later Rh[b]) at 128 + b*2*BR, Rl[b] at 128 + b*2*BR + BR.
+constexpr uint32_t ACC_COLS = 64;
+constexpr uint32_t DBUF0 = 128;
+
+// Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X/Y producer
+// (TMA), 3 = idle, 4..11 = epilogue.  Epilogue warp w reads TMEM lanes
+// 32*(w%4).. (hardware lane quadrant) and the column half (w-4)/4 of each tile.
+template <bool HSIDE, int KP, int NTERMS>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_fused_half(const __grid_constant__ FusedMaps maps, const FusedArgs args)
+{
+    using G = Geo<KP>;
+    constexpr int BR = G::BR;
+    constexpr int QW = BR / 2;          // tile columns handled by one epilogue warp
+    if (args.st && *(volatile const uint32_t *)&args.st->converged) return;
+
+    extern __shared__ unsigned char smem_raw[];
+    uint32_t const base_u32 = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    unsigned char *const base = smem_raw + (base_u32 - smem_u32(smem_raw));
+    unsigned char *const sXh = base;
+    unsigned char *const sXl = base + G::XBYTES;
+    unsigned char *const sY = base + 2 * G::XBYTES;                 // [YST][YSTAGE]
+    unsigned char *const sV = sY + G::YST * G::YSTAGE;              // [VST][VBYTES]
+    uint64_t *const bars = reinterpret_cast<uint64_t *>(sV + G::VST * G::VBYTES);
+    uint64_t *const vfull = bars;                   // [VST]  TMA -> epilogue
+    uint64_t *const vempty = vfull + G::VST;        // [VST]  epilogue -> V producer
+    uint64_t *const yfull = vempty + G::VST;        // [YST]  TMA -> MMA
+    uint64_t *const yempty = yfull + G::YST;        // [YST]  MMA2 commit -> Y producer
+    uint64_t *const dfull = yempty + G::YST;        // [2]    MMA1 commit -> epilogue
+    uint64_t *const rfull = dfull + 2;              // [2]    epilogue -> MMA2
+    uint64_t *const accrdy = rfull + 2;             // [2]    MMA2 commit -> epilogue
+    uint64_t *const xfull = accrdy + 2;             // [1]
+    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xfull + 1);
+    volatile uint32_t *const abort_flag = tmem_slot + 1;
+
+    uint32_t const warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    uint32_t const oblk = blockIdx.x / args.nsplit;
+    uint32_t const split = blockIdx.x % args.nsplit;
+    uint32_t const o0 = oblk * BO;
+    uint32_t const T_all = (args.R + BR - 1) / BR;
+    uint32_t const t_begin = split * args.tiles_per_split;
+    uint32_t const t_end = min(T_all, t_begin + args.tiles_per_split);
+    uint32_t const T = t_end > t_begin ? t_end - t_begin : 0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < G::VST; s++) {
+            mbar_init(&vfull[s], 1);
+            mbar_init(&vempty[s], 8);
+        }
+        for (int s = 0; s < G::YST; s++) {
+            mbar_init(&yfull[s], 1);
+            mbar_init(&yempty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&dfull[b], 1);
+            mbar_init(&rfull[b], 8);
+            mbar_init(&accrdy[b], 1);
+        }
+        mbar_init(xfull, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t const tmem = *tmem_slot;
+
+    if (T == 0 || warp == 3) {
+        // idle
+    } else if (warp == 0) {
+        // ------------------------------------------------------------ V producer
+        if (lane == 0) {
+            for (uint32_t t = 0; t < T; t++) {
+                uint32_t const s = t % G::VST;
+                if (t >= (uint32_t)G::VST &&
+                    !mbar_wait(&vempty[s], ((t / G::VST) - 1) & 1, abort_flag, args.err, 1u))
+                    break;
+                unsigned char *sv = sV + s * G::VBYTES;
+                int const r0 = (int)((t_begin + t) * BR);
+                mbar_expect_tx(&vfull[s], G::VBYTES);
+                if (HSIDE) {
+                    tma_load_2d(sv, &maps.v, &vfull[s], (int)o0, r0);          // V[r0:r0+BR][o0:o0+128]
+                } else {
+#pragma unroll
+                    for (int b = 0; b < BR / 32; b++)                          // V[o0:o0+128][r0+32b : +32]
+                        tma_load_2d(sv + b * (BO * 128), &maps.v, &vfull[s], r0 + 32 * b, (int)o0);
+                }
+            }
+        }
+    } else if (warp == 2) {
+        // ------------------------------------------------------------ X / Y producer
+        if (lane == 0) {
+            mbar_expect_tx(xfull, 2 * G::XBYTES);
+            for (int b = 0; b < G::NB; b++) {
+                tma_load_2d(sXh + b * G::XBLK, &maps.xh, xfull, b * G::CB, (int)o0);
+                tma_load_2d(sXl + b * G::XBLK, &maps.xl, xfull, b * G::CB, (int)o0);
+            }
+            for (uint32_t t = 0; t < T; t++) {
+                uint32_t const s = t % G::YST;
+                if (t >= (uint32_t)G::YST &&
+                    !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 2u))
+                    break;
+                unsigned char *syh = sY + s * G::YSTAGE;
+                unsigned char *syl = syh + G::YBYTES;
+                unsigned char *syth = syl + G::YBYTES;
+                unsigned char *sytl = syth + G::YBYTES;
+                int const r0 = (int)((t_begin + t) * BR);
+                mbar_expect_tx(&yfull[s], G::YSTAGE);
+                for (int b = 0; b < G::NB; b++) {
+                    tma_load_2d(syh + b * G::YBLK, &maps.yh, &yfull[s], b * G::CB, r0);
+                    tma_load_2d(syl + b * G::YBLK, &maps.yl, &yfull[s], b * G::CB, r0);
+                }
+#pragma unroll
+                for (int b = 0; b < BR / 32; b++) {                            // Y^T[0:KP][r0+32b : +32]
+                    tma_load_2d(syth + b * G::YTBLK, &maps.yth, &yfull[s], r0 + 32 * b, 0);
+                    tma_load_2d(sytl + b * G::YTBLK, &maps.ytl, &yfull[s], r0 + 32 * b, 0);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t IDESC1 = idesc_tf32(BO, BR, 0);
+            constexpr uint32_t IDESC2 = idesc_tf32(BO, KP, 0);
+            uint32_t const xh = smem_u32(sXh), xl = smem_u32(sXl);
+            bool ok = mbar_wait(xfull, 0, abort_flag, args.err, 3u);
+            tc_fence_after();
+            // Two issue queues: MMA1 of tile n1 (needs its Y stage and a free D
+            // buffer, i.e. MMA2 of tile n1-2 already issued) and MMA2 of tile n2
+            // (needs the epilogue's R of that tile).  Whichever is ready goes
+            // first, so a late Y stage never holds back the MMA2 that frees a stage.
+            uint32_t n1 = 0, n2 = 0;
+            unsigned long long last = globaltimer();
+            while (ok && n2 < T) {
+                bool progressed = false;
+                if (n1 < T && n1 <= n2 + 1) {
+                    uint32_t const s = n1 % G::YST, b = n1 & 1;
+                    if (mbar_try_wait(&yfull[s], (n1 / G::YST) & 1)) {
+                        tc_fence_after();
+                        uint32_t const yh = smem_u32(sY + s * G::YSTAGE);
+                        uint32_t const yl = yh + G::YBYTES;
+                        uint32_t const dcol = tmem + DBUF0 + b * 2 * BR;
+                        // MMA1: D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
+                        uint32_t acc = 0;
+#pragma unroll
+                        for (int tt = 0; tt < NTERMS; tt++) {
+                            int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
+                            uint32_t const xa = (term == 2) ? xl : xh;
+                            uint32_t const yb = (term == 1) ? yl : yh;
+#pragma unroll
+                            for (int ks = 0; ks < KP / 8; ks++) {
+                                int const blk = ks / (G::CB / 8), within = (ks % (G::CB / 8)) * 32;
+                                uint64_t const ad = smem_desc(xa + blk * G::XBLK + within, 16, 8 * G::ROWB, G::LAYOUT);
+                                uint64_t const bd = smem_desc(yb + blk * G::YBLK + within, 16, 8 * G::ROWB, G::LAYOUT);
+                                mma_ss(dcol, ad, bd, IDESC1, acc);
+                                acc = 1;
+                            }
+                        }
+                        tc_commit(&dfull[b]);
+                        n1++;
+                        progressed = true;
+                    }
+                }
+                if (n2 < n1) {
+                    uint32_t const sp = n2 % G::YST, bp = n2 & 1;
+                    if (mbar_try_wait(&rfull[bp], (n2 >> 1) & 1)) {
+                        tc_fence_after();
+                        uint32_t const yth = smem_u32(sY + sp * G::YSTAGE + 2 * G::YBYTES);
+                        uint32_t const ytl = yth + G::YBYTES;
+                        uint32_t const rh = tmem + DBUF0 + bp * 2 * BR;
+                        uint32_t const rl = rh + BR;
+                        // MMA2: Acc[bp] = Rl Yh + Rh Yl + Rh Yh for this tile only; B = Y^T
+                        // (KP rows, K-major), K = BR reduction rows in steps of 8.  Tiles
+                        // are summed by the epilogue in FP32 registers.
+                        uint32_t acc = 0;
+#pragma unroll
+                        for (int tt = 0; tt < NTERMS; tt++) {
+                            int const term = NTERMS - 1 - tt;
+                            uint32_t const ra = (term == 2) ? rl : rh;
+                            uint32_t const yb = (term == 1) ? ytl : yth;
+#pragma unroll
+                            for (int ks = 0; ks < BR / 8; ks++) {
+                                uint64_t const bd = smem_desc(yb + (ks / 4) * G::YTBLK + (ks % 4) * 32, 16, 1024, 2u);
+                                mma_ts(tmem + bp * ACC_COLS, ra + ks * 8, bd, IDESC2, acc);
+                                acc = 1;
+                            }
+                        }
+                        tc_commit(&yempty[sp]);
+                        tc_commit(&accrdy[bp]);
+                        n2++;
+                        progressed = true;
+                    }
+                }
+                if (progressed) {
+                    last = globaltimer();
+                } else if (*abort_flag) {
+                    ok = false;
+                } else if (globaltimer() - last > WAIT_LIMIT_NS) {
+                    *abort_flag = 1;
+                    atomicExch(args.err, 4u);
+                    ok = false;
+                }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        uint32_t const quad = warp & 3;
+        uint32_t const half = (warp - 4) >> 2;         // 0 or 1
+        uint32_t const row = quad * 32 + lane;        // TMEM lane = output row within the block
+        uint32_t const lane_addr = tmem + ((quad * 32) << 16);
+        float sum[G::HALF];
+#pragma unroll
+        for (int c = 0; c < G::HALF; c++) sum[c] = 0.0f;
+        bool ok = true;
+        for (uint32_t t = 0; t <= T && ok; t++) {
+            if (t < T) {
+                uint32_t const s = t % G::VST, b = t & 1;
+                if (!mbar_wait(&dfull[b], (t >> 1) & 1, abort_flag, args.err, 6u)) { ok = false; break; }
+                if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) { ok = false; break; }
+                tc_fence_after();
+                const unsigned char *sv = sV + s * G::VBYTES;
+                uint32_t const dcol = DBUF0 + b * 2 * BR + half * QW;
+                uint32_t d[32];
+                if (QW == 32)
+                    tmem_ld32(lane_addr + dcol, d);
+                else
+                    tmem_ld16(lane_addr + dcol, d);
+                float v[32];
+                if (HSIDE) {
+                    // V tile [BR rows][128 cols], row-major; this thread's column = row.
+                    const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
+#pragma unroll
+                    for (int c = 0; c < QW; c++) v[c] = vs[c * BO];
+                } else {
+                    // V box `half` (BR == 64) or half a box (BR == 32): [128 rows][32 floats], 128B swizzle.
+                    int const qb = (BR == 64) ? half : 0;
+                    int const c0 = (BR == 64) ? 0 : half * 4;   // 16-byte chunk offset
+                    const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
+#pragma unroll
+                    for (int c = 0; c < 32 / 4; c++) {
+                        if (c >= QW / 4) break;
+                        float4 const x = *reinterpret_cast<const float4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
+                        v[4 * c + 0] = x.x;
+                        v[4 * c + 1] = x.y;
+                        v[4 * c + 2] = x.z;
+                        v[4 * c + 3] = x.w;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
+                tmem_wait_ld_dep(d);
+                uint32_t hi[32], lo[32];
+#pragma unroll
+                for (int c = 0; c < QW; c++) {
+                    float const r = (v[c] == 0.0f) ? 0.0f : __fdividef(v[c], __uint_as_float(d[c]));
+                    float const h = tf32_rna(r);
+                    hi[c] = __float_as_uint(h);
+                    lo[c] = __float_as_uint(r - h);
+                }
+#ifdef NMFB_FUSED_DEBUG
+                if (args.dbg && blockIdx.x == 0 && t == 0)
+                    for (int c = 0; c < QW; c++) {
+                        args.dbg[row * 64 + half * QW + c] = __uint_as_float(d[c]);
+                        args.dbg[BO * 64 + row * 64 + half * QW + c] = v[c];
+                        args.dbg[2 * BO * 64 + row * 64 + half * QW + c] = __uint_as_float(hi[c]);
+                    }
+#endif
+                if (QW == 32) {
+                    tmem_st32(lane_addr + dcol, hi);
+                    if (NTERMS == 3) tmem_st32(lane_addr + dcol + BR, lo);
+                } else {
+                    tmem_st16(lane_addr + dcol, hi);
+                    if (NTERMS == 3) tmem_st16(lane_addr + dcol + BR, lo);
+                }
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&rfull[b]);
+            }
+            if (t >= 1) {
+                // Add the previous tile's accumulator (TMEM) into the FP32 registers.
+                uint32_t const tp = t - 1, bp = tp & 1;
+                if (!mbar_wait(&accrdy[bp], (tp >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
+                tc_fence_after();
+                uint32_t a[32];
+                if (G::HALF == 32)
+                    tmem_ld32(lane_addr + bp * ACC_COLS + half * G::HALF, a);
+                else if (G::HALF == 16)
+                    tmem_ld16(lane_addr + bp * ACC_COLS + half * G::HALF, a);
+                else
+                    tmem_ld8(lane_addr + bp * ACC_COLS + half * G::HALF, a);
+                tmem_wait_ld_dep(a);
+#pragma unroll
+                for (int c = 0; c < G::HALF; c++) sum[c] += __uint_as_float(a[c]);
+            }
+        }
+        if (ok) {
+            uint32_t const o = o0 + row;
+#ifdef NMFB_FUSED_DEBUG
+            if (args.dbg && blockIdx.x == 0)
+                for (int c = 0; c < G::HALF; c++) args.dbg[3 * BO * 64 + row * KP + half * G::HALF + c] = sum[c];
+#endif
+            if (o < args.O) {
+                float *dst = args.part + ((size_t)split * args.O + o) * KP + half * G::HALF;
+#pragma unroll
+                for (int c = 0; c < G::HALF; c += 4)
+                    *reinterpret_cast<float4 *>(dst + c) = make_float4(sum[c], sum[c + 1], sum[c + 2], sum[c + 3]);
+            }
+        }
+    }
+    if (T == 0 && warp >= 4) {
+        uint32_t const o = o0 + (warp & 3) * 32 + lane;
+        uint32_t const half = (warp - 4) >> 2;
+        if (o < args.O) {
+            float *dst = args.part + ((size_t)split * args.O + o) * KP + half * G::HALF;
+            for (int c = 0; c < G::HALF; c++) dst[c] = 0.0f;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int encode_2d(nmfb_ctx *ctx, CUtensorMap *map, const float *base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+              uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw)
+{
+    auto fn = encode_fn();
+    if (!fn) return nmfb_fail(ctx, NMFB_ENODEV, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {row_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nmfb_fail(ctx, NMFB_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return NMFB_OK;
+}
+
+struct FusedPlan {
+    FusedMaps mapsH, mapsW;  // update_H (HSIDE) and update_W
+    uint32_t *dErr;
+#ifdef NMFB_FUSED_DEBUG
+    float *dDbg;
+#endif
+};
+
+template <bool HSIDE, int KP, int NTERMS>
+int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
+{
+    using G = Geo<KP>;
+    constexpr int BR = G::BR;
+    auto kern = k_fused_half<HSIDE, KP, NTERMS>;
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    uint32_t const O = HSIDE ? ctx->m : ctx->n;
+    uint32_t const R = HSIDE ? ctx->n : ctx->m;
+    uint32_t const oblocks = (O + BO - 1) / BO;
+    uint32_t const T = (R + BR - 1) / BR;
+    // Splits of the reduction so that the grid fills the GPU a few times over.
+    uint32_t want = (4u * (uint32_t)ctx->sm_count + oblocks - 1) / oblocks;
+    if (want < 1) want = 1;
+    if (want > NMFB_MAX_SPLIT) want = NMFB_MAX_SPLIT;
+    uint32_t tps = (T + want - 1) / want;
+    if (tps < 4) tps = T < 4 ? T : 4;
+    uint32_t const nsplit = (T + tps - 1) / tps;
+    if ((size_t)nsplit * O * KP > ctx->part_items)
+        return nmfb_fail(ctx, NMFB_EINVAL, "fused: partial buffer too small (%u splits)", nsplit);
+    FusedArgs args;
+    args.O = O;
+    args.R = R;
+    args.tiles_per_split = tps;
+    args.nsplit = nsplit;
+    args.part = ctx->dPart;
+    args.err = plan->dErr;
+    args.st = ctx->dState;
+#ifdef NMFB_FUSED_DEBUG
+    args.dbg = plan->dDbg;
+#endif
+    int const main = HSIDE ? 0 : 1;
+    int rc = nmfb_prof_begin(ctx, main);
+    if (rc) return rc;
+    kern<<<oblocks * nsplit, NTHREADS, G::SMEM, ctx->stream>>>(maps, args);
+    NMFB_LAUNCH_CHECK(ctx);
+    if ((rc = nmfb_prof_end(ctx, main))) return rc;
+    return (int)nsplit;
+}
+
+template <bool HSIDE>
+int dispatch(nmfb_ctx *ctx, const FusedMaps &maps)
+{
+    bool const x3 = ctx->arm == NMFB_ARM_FUSED;
+    switch (ctx->kp) {
+    case 16: return x3 ? launch_fused<HSIDE, 16, 3>(ctx, maps) : launch_fused<HSIDE, 16, 1>(ctx, maps);
+    case 32: return x3 ? launch_fused<HSIDE, 32, 3>(ctx, maps) : launch_fused<HSIDE, 32, 1>(ctx, maps);
+    case 64: return x3 ? launch_fused<HSIDE, 64, 3>(ctx, maps) : launch_fused<HSIDE, 64, 1>(ctx, maps);
+    default: return nmfb_fail(ctx, NMFB_EINVAL, "fused arm: unsupported padded rank %u", ctx->kp);
+    }
+}
+
+int fused_half(nmfb_ctx *ctx, bool is_H, int adjust)
+{
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    if (!plan) return nmfb_fail(ctx, NMFB_ESTATE, "fused arm not prepared");
+    float *X = is_H ? ctx->dH : ctx->dW;
+    const float *Y = is_H ? ctx->dW : ctx->dH;
+    uint32_t const xrows = is_H ? ctx->m : ctx->n;
+    uint32_t const yrows = is_H ? ctx->n : ctx->m;
+    float *acc = is_H ? ctx->dAccW : ctx->dAccH;
+    int const whole = is_H ? 2 : 3;
+    int rc = nmfb_prof_begin(ctx, whole);
+    if (rc) return rc;
+    if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
+    int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH) : dispatch<false>(ctx, plan->mapsW);
+    if (nsplit < 0) return nsplit;
+    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust,
+                     is_H ? &ctx->sH : &ctx->sW);
+    if (rc) return rc;
+    return nmfb_prof_end(ctx, whole);
+}
+
+}  // namespace
+
+template <int KP>
+int set_smem_attrs(nmfb_ctx *ctx)
+{
+    int const smem = Geo<KP>::SMEM;
+    NMFB_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fused_half<true, KP, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    NMFB_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fused_half<false, KP, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    NMFB_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fused_half<true, KP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    NMFB_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fused_half<false, KP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return NMFB_OK;
+}
+
+int nmfb_fused_prepare(nmfb_ctx *ctx)
+{
+    if (ctx->tmaps) return NMFB_OK;
+    uint32_t const kp = ctx->kp;
+    if (kp != 16 && kp != 32 && kp != 64)
+        return nmfb_fail(ctx, NMFB_EINVAL, "the fused arm supports ranks up to 64 (k=%u); use the plain arm", ctx->k);
+    int rc = (kp == 16) ? set_smem_attrs<16>(ctx) : (kp == 32) ? set_smem_attrs<32>(ctx) : set_smem_attrs<64>(ctx);
+    if (rc) return rc;
+    FusedPlan *plan = (FusedPlan *)calloc(1, sizeof(FusedPlan));
+    if (!plan) return nmfb_fail(ctx, NMFB_ENOMEM, "fused plan");
+    ctx->tmaps = plan;
+    cudaError_t e = cudaMalloc((void **)&plan->dErr, sizeof(uint32_t));
+    if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused error word: %s", cudaGetErrorString(e));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
+#ifdef NMFB_FUSED_DEBUG
+    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (3 * BO * 64 + BO * 64) * sizeof(float)));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (3 * BO * 64 + BO * 64) * sizeof(float), ctx->stream));
+#endif
+    uint32_t const cb = (kp == 16) ? 16 : 32;
+    CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    uint64_t const vrow = ctx->ldv * sizeof(float), frow = (uint64_t)kp * sizeof(float);
+    uint32_t const br = (kp >= 64) ? 32 : 64;
+    const nmfb::Split &W = ctx->sW, &H = ctx->sH;
+    // update_H: X = H (rows m), Y = W (rows n); V tile [br rows of V][128 cols].
+    FusedMaps &mh = plan->mapsH;
+    if ((rc = encode_2d(ctx, &mh.v, ctx->dV, ctx->m, ctx->n, vrow, BO, br, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
+    if ((rc = encode_2d(ctx, &mh.xh, H.hi, kp, ctx->m, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.xl, H.lo, kp, ctx->m, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.yh, W.hi, kp, ctx->n, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.yl, W.lo, kp, ctx->n, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.yth, W.hiT, ctx->n, kp, W.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode_2d(ctx, &mh.ytl, W.loT, ctx->n, kp, W.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    // update_W: X = W (rows n), Y = H (rows m); V tile [128 rows][32 cols] x (br/32), 128B swizzle.
+    FusedMaps &mw = plan->mapsW;
+    if ((rc = encode_2d(ctx, &mw.v, ctx->dV, ctx->m, ctx->n, vrow, 32, BO, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode_2d(ctx, &mw.xh, W.hi, kp, ctx->n, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.xl, W.lo, kp, ctx->n, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.yh, H.hi, kp, ctx->m, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.yl, H.lo, kp, ctx->m, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.yth, H.hiT, ctx->m, kp, H.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode_2d(ctx, &mw.ytl, H.loT, ctx->m, kp, H.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    return NMFB_OK;
+}
+
+int nmfb_fused_release(nmfb_ctx *ctx)
+{
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    if (!plan) return NMFB_OK;
+    if (plan->dErr) cudaFree(plan->dErr);
+    free(plan);
+    ctx->tmaps = nullptr;
+    return NMFB_OK;
+}
+
+int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust) { return fused_half(ctx, true, adjust); }
+int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust) { return fused_half(ctx, false, adjust); }
+
+int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
+{
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    *code = 0;
+    if (!plan) return NMFB_OK;
+    NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(code, plan->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return NMFB_OK;
+}
+
+#ifdef NMFB_FUSED_DEBUG
+extern "C" int nmfb_debug_dump(nmfb_ctx *ctx, float *host)
+{
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    NMFB_CUDA_TRY(ctx, cudaMemcpy(host, plan->dDbg, (3 * BO * 64 + BO * 64) * sizeof(float), cudaMemcpyDeviceToHost));
+    return NMFB_OK;
+}
+#endif

@@ -45,8 +45,9 @@ int dev_alloc(nmfb_ctx *ctx, T **p, size_t items, const char *what)
 void free_all(nmfb_ctx *ctx)
 {
     void *bufs[] = {ctx->dV,   ctx->dW,    ctx->dH,     ctx->dAccW,  ctx->dAccH,  ctx->dWH,    ctx->dPart,
-                    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->dWhi, ctx->dWlo, ctx->dHhi,
-                    ctx->dHlo, ctx->dLabels, ctx->dFirst, ctx->dLastRep, ctx->dState};
+                    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->sW.hi, ctx->sW.lo, ctx->sW.hiT,
+                    ctx->sW.loT, ctx->sH.hi, ctx->sH.lo, ctx->sH.hiT, ctx->sH.loT, ctx->dLabels, ctx->dFirst,
+                    ctx->dLastRep, ctx->dState};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->hState) cudaFreeHost(ctx->hState);
@@ -94,10 +95,10 @@ int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, 
 
 int refresh_splits(nmfb_ctx *ctx)
 {
-    if (!ctx->dWhi) return NMFB_OK;
-    int rc = nmfb_split_tf32(ctx, ctx->dW, ctx->n, ctx->dWhi, ctx->dWlo);
+    if (!ctx->sW.hi) return NMFB_OK;
+    int rc = nmfb_split_tf32(ctx, ctx->dW, ctx->n, &ctx->sW);
     if (rc) return rc;
-    return nmfb_split_tf32(ctx, ctx->dH, ctx->m, ctx->dHhi, ctx->dHlo);
+    return nmfb_split_tf32(ctx, ctx->dH, ctx->m, &ctx->sH);
 }
 
 int do_update_H(nmfb_ctx *ctx, int adjust)
@@ -187,13 +188,9 @@ int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, 
     if ((rc = dev_alloc(ctx, &ctx->dH, (size_t)m * kp, "H"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dAccW, kp, "accW"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dAccH, kp, "accH"))) return rc;
-    // Split-reduction partials: the plans never exceed 2*SMs blocks of 64 outputs.
-    ctx->part_items = (size_t)NMFB_MAX_SPLIT * maxr * kp;
-    {
-        size_t const cap = (size_t)(2 * ctx->sm_count + 2) * 64 * kp + 2 * maxr * kp;
-        if (ctx->part_items > cap) ctx->part_items = cap;
-        if (ctx->part_items < 2 * maxr * kp) ctx->part_items = 2 * maxr * kp;
-    }
+    // Split-reduction partials: both arms size their splits so that
+    // nsplit * rows <= 4*SMs*128 + 2*rows + 128 (see the split planners).
+    ctx->part_items = ((size_t)512 * ctx->sm_count + 2 * maxr + 256) * kp;
     if ((rc = dev_alloc(ctx, &ctx->dPart, ctx->part_items, "partials"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dColPart, (size_t)2 * 1024 * kp, "colsum partials"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dTickets, 16, "tickets"))) return rc;
@@ -219,20 +216,31 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
     if (rc) return rc;
     if (arm != NMFB_ARM_FUSED && arm != NMFB_ARM_PLAIN && arm != NMFB_ARM_FUSED_TF32)
         return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
-    ctx->arm = arm;
     if (arm == NMFB_ARM_PLAIN) {
         if (!ctx->dWH && (rc = dev_alloc(ctx, &ctx->dWH, (size_t)ctx->n * ctx->ldv, "WH"))) return rc;
+        ctx->arm = arm;
         return NMFB_OK;
     }
-    if (!ctx->dWhi) {
+    if (ctx->kp > 64)
+        return nmfb_fail(ctx, NMFB_EINVAL, "the fused arms support ranks up to 64 (k=%u); use NMFB_ARM_PLAIN", ctx->k);
+    if (!ctx->sW.hi) {
         size_t const kp = ctx->kp;
-        if ((rc = dev_alloc(ctx, &ctx->dWhi, (size_t)ctx->n * kp, "Whi"))) return rc;
-        if ((rc = dev_alloc(ctx, &ctx->dWlo, (size_t)ctx->n * kp, "Wlo"))) return rc;
-        if ((rc = dev_alloc(ctx, &ctx->dHhi, (size_t)ctx->m * kp, "Hhi"))) return rc;
-        if ((rc = dev_alloc(ctx, &ctx->dHlo, (size_t)ctx->m * kp, "Hlo"))) return rc;
-        if ((rc = refresh_splits(ctx))) return rc;
+        struct { nmfb::Split *s; uint32_t rows; const char *name; } f[2] = {{&ctx->sW, ctx->n, "W"}, {&ctx->sH, ctx->m, "H"}};
+        for (auto &x : f) {
+            x.s->ldT = ((size_t)x.rows + 31) / 32 * 32;
+            if ((rc = dev_alloc(ctx, &x.s->hi, (size_t)x.rows * kp, x.name))) return rc;
+            if ((rc = dev_alloc(ctx, &x.s->lo, (size_t)x.rows * kp, x.name))) return rc;
+            if ((rc = dev_alloc(ctx, &x.s->hiT, kp * x.s->ldT, x.name))) return rc;
+            if ((rc = dev_alloc(ctx, &x.s->loT, kp * x.s->ldT, x.name))) return rc;
+            NMFB_CUDA_TRY(ctx, cudaMemsetAsync(x.s->hiT, 0, kp * x.s->ldT * sizeof(float), ctx->stream));
+            NMFB_CUDA_TRY(ctx, cudaMemsetAsync(x.s->loT, 0, kp * x.s->ldT * sizeof(float), ctx->stream));
+        }
     }
-    return nmfb_fused_prepare(ctx);
+    // W and H may have been changed by another arm: refresh their TF32 splits.
+    if ((rc = refresh_splits(ctx))) return rc;
+    if ((rc = nmfb_fused_prepare(ctx))) return rc;
+    ctx->arm = arm;
+    return NMFB_OK;
 }
 
 int nmfb_destroy(nmfb_ctx *ctx)
@@ -412,6 +420,11 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
     if (rc) return rc;
+    {
+        uint32_t code = 0;
+        if ((rc = nmfb_fused_error(ctx, &code))) return rc;
+        if (code) return nmfb_fail(ctx, NMFB_ETIMEOUT, "fused kernel: bounded wait expired (site %u)", code);
+    }
     if (converged) *converged = fin.converged ? 1 : 0;
     if (iterations) *iterations = fin.converged ? fin.conv_tests * niter_test_conv : n_iters;
     return NMFB_OK;
@@ -545,6 +558,9 @@ int nmfb_synchronize(nmfb_ctx *ctx)
     int rc = check_ctx(ctx);
     if (rc) return rc;
     NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    uint32_t code = 0;
+    if ((rc = nmfb_fused_error(ctx, &code))) return rc;
+    if (code) return nmfb_fail(ctx, NMFB_ETIMEOUT, "fused kernel: bounded wait expired (site %u)", code);
     return NMFB_OK;
 }
 

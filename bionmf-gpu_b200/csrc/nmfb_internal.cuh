@@ -23,10 +23,11 @@ struct ConvState {
     uint32_t pad;
 };
 
-// Scratch for one deterministic column-sum reduction.
-struct ColsumScratch {
-    double *part;        // [blocks][kp]
-    uint32_t *ticket;
+// TF32 hi/lo split of one factor for the tensor-core arms: row-major
+// (rows x kp) and transposed (kp x ldT, ldT = rows rounded up to 32).
+struct Split {
+    float *hi, *lo, *hiT, *loT;
+    size_t ldT;
 };
 
 }  // namespace nmfb
@@ -50,8 +51,8 @@ struct nmfb_ctx {
     double *dObj;          // objective partials + results
     uint32_t *dObjTicket;
 
-    // tcgen05 arm: hi/lo tf32 splits of the factors (row-major, kp columns).
-    float *dWhi, *dWlo, *dHhi, *dHlo;
+    // tcgen05 arms: TF32 hi/lo splits of the factors (null for the plain arm).
+    nmfb::Split sW, sH;
     int sm_count;
     void *tmaps;           // fused-arm tensor maps (host copy), see kernels_fused.cu
 
@@ -102,13 +103,13 @@ extern "C" int nmfb_prof_end(nmfb_ctx *ctx, int cls);
 // ---- kernels_common.cu ----------------------------------------------------
 int nmfb_colsum(nmfb_ctx *ctx, const float *X, uint32_t rows, float *acc, int which);
 int nmfb_muldiv(nmfb_ctx *ctx, float *X, uint32_t rows, const float *part, uint32_t nsplit,
-                size_t split_stride, const float *acc, int adjust, float *hi, float *lo);
+                size_t split_stride, const float *acc, int adjust, const nmfb::Split *split);
 int nmfb_adjust_rows(nmfb_ctx *ctx, float *X, uint32_t rows);
 int nmfb_classify_and_test(nmfb_ctx *ctx, uint32_t niter_test_conv);
 int nmfb_classify_only(nmfb_ctx *ctx);
 int nmfb_reset_conv(nmfb_ctx *ctx, uint32_t stop_threshold);
 int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl);
-int nmfb_split_tf32(nmfb_ctx *ctx, const float *X, uint32_t rows, float *hi, float *lo);
+int nmfb_split_tf32(nmfb_ctx *ctx, float *X, uint32_t rows, const nmfb::Split *split);
 
 // ---- kernels_plain.cu -----------------------------------------------------
 int nmfb_plain_update_H(nmfb_ctx *ctx, int adjust);
@@ -119,6 +120,7 @@ int nmfb_fused_prepare(nmfb_ctx *ctx);
 int nmfb_fused_release(nmfb_ctx *ctx);
 int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust);
+int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code);
 
 // Max number of reduction splits used by any arm (sizes dPart).
 #define NMFB_MAX_SPLIT 64

@@ -144,6 +144,11 @@ def test_engine_matches_reference_fixture(pkg, oracle, case, arm):
     g = load_golden(case)
     V = g["V"]
     k = int(g["k"])
+    if arm == "fused" and k > 64:
+        with pytest.raises(pkg.NMFError) as ei:        # fused arms cover k <= 64
+            pkg.NMF(V.shape[0], V.shape[1], k, arm=arm)
+        assert ei.value.code == -1
+        return
     with _engine(pkg, V, k, arm, seed=int(g["seed"])) as e:
         it, conv = e.run(int(g["n_iters"]), int(g["niter_test_conv"]), int(g["stop_threshold"]))
         assert it == int(g["iterations"]) and conv == bool(g["converged"])
