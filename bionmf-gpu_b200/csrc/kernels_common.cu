@@ -1,7 +1,6 @@
 // kernels_common.cu -- small kernels shared by every update arm:
 //   * deterministic column sums of W / H            (reference: matrix_to_row)
-//   * mul-div update with fused EPS adjust and TF32 hi/lo split
-//                                                   (reference: matrix_mul_div + matrix_adjust)
+//   * mul-div update with fused EPS adjust       (reference: matrix_mul_div + matrix_adjust)
 //   * classification (argmax) + device-side connectivity test and stop rule
 //                                                   (reference: get_classification + get_difference)
 //   * FP64 objective reductions (||V||^2, ||V-WH||^2, KL divergence)
@@ -28,13 +27,6 @@ int nmfb_fail(nmfb_ctx *ctx, int code, const char *fmt, ...)
 namespace {
 
 __device__ __forceinline__ bool halted(const ConvState *st) { return st && *(volatile const uint32_t *)&st->converged; }
-
-__device__ __forceinline__ float tf32_rna(float x)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
 
 // EPS adjust of the reference (src/GPU_kernels.cu:2338-2345): fmaxf(x, FLT_MIN),
 // which also maps NaN to FLT_MIN.
@@ -84,69 +76,36 @@ __global__ void k_colsum(const float *__restrict__ X, uint32_t rows, uint32_t kp
 }
 
 // ---------------------------------------------------------------------------
-// Factor update over tiles of 32 rows (one block per tile, grid-stride):
-//   mode FU_SPLIT : v = X[r][c]                                  (refresh splits)
+// Factor update, one thread per entry of X (rows x kp):
 //   mode FU_MULDIV: v = (X[r][c] * sum_s part[s][r][c]) / acc[c]  (matrix_mul_div,
-//                   src/GPU_kernels.cu:2013-2019: product first, then the division)
-//   mode FU_ADJUST: v = fmaxf(X[r][c], FLT_MIN)                   (matrix_adjust)
-// then, for MULDIV, the optional EPS adjust.  Padding columns c >= k are 0.
-// When a Split is given, also writes v's TF32 hi/lo parts row-major and,
-// through a shared-memory transpose, column-major (coalesced both ways).
-enum { FU_SPLIT = 0, FU_MULDIV = 1, FU_ADJUST = 2 };
+//                   src/GPU_kernels.cu:2013-2019: product first, then the division),
+//                   followed by the EPS adjust when `adjust` is set;
+//   mode FU_ADJUST: v = fmaxf(X[r][c], FLT_MIN)                   (matrix_adjust).
+// Padding columns c >= k are kept at 0.  The split partials are summed in
+// split order, so the result does not depend on scheduling.
+enum { FU_MULDIV = 1, FU_ADJUST = 2 };
 
 __global__ void __launch_bounds__(256) k_factor(int mode, float *__restrict__ X, uint32_t rows, uint32_t kp, uint32_t k,
                                                 const float *__restrict__ part, uint32_t nsplit, size_t split_stride,
-                                                const float *__restrict__ acc, int adjust, nmfb::Split sp,
-                                                const ConvState *st)
+                                                const float *__restrict__ acc, int adjust, const ConvState *st)
 {
     if (halted(st)) return;
-    __shared__ float tH[64][33];
-    __shared__ float tL[64][33];
-    bool const has_split = sp.hi != nullptr;
-    uint32_t const ntiles = (rows + 31) / 32;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t const r0 = tile * 32;
-        for (uint32_t cg = 0; cg < kp; cg += 64) {
-            uint32_t const kc = min(64u, kp - cg);
-            for (uint32_t e = threadIdx.x; e < 32 * kc; e += blockDim.x) {
-                uint32_t const rr = e / kc, c = cg + e % kc, r = r0 + rr;
-                if (r >= rows) continue;
-                size_t const idx = (size_t)r * kp + c;
-                float v = 0.0f;
-                if (c < k) {
-                    if (mode == FU_MULDIV) {
-                        float s = 0.0f;
-                        for (uint32_t q = 0; q < nsplit; q++) s += part[q * split_stride + idx];
-                        v = __fdiv_rn(X[idx] * s, acc[c]);
-                        if (adjust) v = adjust_value(v);
-                    } else if (mode == FU_ADJUST) {
-                        v = adjust_value(X[idx]);
-                    } else {
-                        v = X[idx];
-                    }
-                }
-                if (mode != FU_SPLIT) X[idx] = v;
-                if (has_split) {
-                    float const h = tf32_rna(v);
-                    sp.hi[idx] = h;
-                    sp.lo[idx] = v - h;
-                    tH[c - cg][rr] = h;
-                    tL[c - cg][rr] = v - h;
-                }
-            }
-            if (has_split) {
-                __syncthreads();
-                for (uint32_t e = threadIdx.x; e < 32 * kc; e += blockDim.x) {
-                    uint32_t const cc = e / 32, rr = e % 32, r = r0 + rr;
-                    if (r < rows) {
-                        size_t const o = (size_t)(cg + cc) * sp.ldT + r;
-                        sp.hiT[o] = tH[cc][rr];
-                        sp.loT[o] = tL[cc][rr];
-                    }
-                }
-                __syncthreads();
+    size_t const total = (size_t)rows * kp;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        uint32_t const c = (uint32_t)(idx % kp);
+        float v = 0.0f;
+        if (c < k) {
+            if (mode == FU_MULDIV) {
+                float s = 0.0f;
+                for (uint32_t q = 0; q < nsplit; q++) s += part[q * split_stride + idx];
+                v = __fdiv_rn(X[idx] * s, acc[c]);
+                if (adjust) v = adjust_value(v);
+            } else {
+                v = adjust_value(X[idx]);
             }
         }
+        X[idx] = v;
     }
 }
 
@@ -162,7 +121,7 @@ __global__ void __launch_bounds__(256) k_factor(int mode, float *__restrict__ X,
 // before get_classification in the reference, src/NMF_GPU.c:611-655).
 // Also records first[label] = min sample index per label (canonical partition).
 __global__ void k_classify(float *__restrict__ H, uint32_t m, uint32_t kp, uint32_t k, uint32_t bdx,
-                           int adjust, nmfb::Split sp, uint32_t *__restrict__ labels, uint32_t *__restrict__ first,
+                           int adjust, uint32_t *__restrict__ labels, uint32_t *__restrict__ first,
                            const ConvState *st)
 {
     if (halted(st)) return;
@@ -179,15 +138,7 @@ __global__ void k_classify(float *__restrict__ H, uint32_t m, uint32_t kp, uint3
     if (adjust && valid) {
         for (uint32_t c = t; c < kp; c += bdx) {
             if (c >= k) continue;
-            float const v = adjust_value(row[c]);
-            row[c] = v;
-            if (sp.hi) {
-                float const h = tf32_rna(v);
-                sp.hi[(size_t)j * kp + c] = h;
-                sp.lo[(size_t)j * kp + c] = v - h;
-                sp.hiT[(size_t)c * sp.ldT + j] = h;
-                sp.loT[(size_t)c * sp.ldT + j] = v - h;
-            }
+            row[c] = adjust_value(row[c]);
         }
         __syncwarp();
     }
@@ -346,34 +297,24 @@ int nmfb_colsum(nmfb_ctx *ctx, const float *X, uint32_t rows, float *acc, int wh
 }
 
 static int launch_factor(nmfb_ctx *ctx, int mode, float *X, uint32_t rows, const float *part, uint32_t nsplit,
-                         size_t split_stride, const float *acc, int adjust, const nmfb::Split *split,
-                         const ConvState *st)
+                         size_t split_stride, const float *acc, int adjust, const ConvState *st)
 {
-    nmfb::Split sp = split ? *split : nmfb::Split{nullptr, nullptr, nullptr, nullptr, 0};
-    unsigned const tiles = (rows + 31) / 32;
-    unsigned const grid = tiles < 8u * (unsigned)ctx->sm_count ? tiles : 8u * (unsigned)ctx->sm_count;
-    k_factor<<<grid, 256, 0, ctx->stream>>>(mode, X, rows, ctx->kp, ctx->k, part, nsplit, split_stride, acc, adjust,
-                                           sp, st);
+    size_t const total = (size_t)rows * ctx->kp;
+    unsigned const grid = grid_for(total, 256, 8u * (unsigned)ctx->sm_count);
+    k_factor<<<grid, 256, 0, ctx->stream>>>(mode, X, rows, ctx->kp, ctx->k, part, nsplit, split_stride, acc, adjust, st);
     NMFB_LAUNCH_CHECK(ctx);
     return NMFB_OK;
 }
 
 int nmfb_muldiv(nmfb_ctx *ctx, float *X, uint32_t rows, const float *part, uint32_t nsplit, size_t split_stride,
-                const float *acc, int adjust, const nmfb::Split *split)
+                const float *acc, int adjust)
 {
-    return launch_factor(ctx, FU_MULDIV, X, rows, part, nsplit, split_stride, acc, adjust, split, ctx->dState);
+    return launch_factor(ctx, FU_MULDIV, X, rows, part, nsplit, split_stride, acc, adjust, ctx->dState);
 }
 
 int nmfb_adjust_rows(nmfb_ctx *ctx, float *X, uint32_t rows)
 {
-    const nmfb::Split *sp = nullptr;
-    if (ctx->sW.hi) sp = (X == ctx->dW) ? &ctx->sW : &ctx->sH;
-    return launch_factor(ctx, FU_ADJUST, X, rows, nullptr, 0, 0, nullptr, 0, sp, nullptr);
-}
-
-int nmfb_split_tf32(nmfb_ctx *ctx, float *X, uint32_t rows, const nmfb::Split *split)
-{
-    return launch_factor(ctx, FU_SPLIT, X, rows, nullptr, 0, 0, nullptr, 0, split, nullptr);
+    return launch_factor(ctx, FU_ADJUST, X, rows, nullptr, 0, 0, nullptr, 0, nullptr);
 }
 
 static uint32_t classify_width(uint32_t k)
@@ -392,8 +333,8 @@ static int launch_classify(nmfb_ctx *ctx, int adjust, const ConvState *st)
     uint32_t const groups = block / bdx;
     uint32_t const grid = (ctx->m + groups - 1) / groups;
     size_t const smem = (size_t)block * (sizeof(float) + sizeof(uint32_t));
-    k_classify<<<grid, block, smem, ctx->stream>>>(ctx->dH, ctx->m, ctx->kp, ctx->k, bdx, adjust, ctx->sH,
-                                                  ctx->dLabels, ctx->dFirst, st);
+    k_classify<<<grid, block, smem, ctx->stream>>>(ctx->dH, ctx->m, ctx->kp, ctx->k, bdx, adjust, ctx->dLabels,
+                                                  ctx->dFirst, st);
     NMFB_LAUNCH_CHECK(ctx);
     return NMFB_OK;
 }

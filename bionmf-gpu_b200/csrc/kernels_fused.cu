@@ -5,28 +5,34 @@
 // dimension, the partial  Xaux = sum_r  (V ./ (X Y^T))[o][r] * Y[r][:]
 // without ever materialising the n x m quotient:
 //
-//   TMA      : V tile (128 x BR, FP32), Y tile (BR x KP) and its transpose
-//              Y^T tile (KP x BR), each as TF32 hi and lo parts, into a
-//              STAGES-deep shared-memory ring; X (128 x KP, hi/lo) once.
-//   MMA1     : D (TMEM, 128 x BR, FP32) = Xh Yh^T + Xh Yl^T + Xl Yh^T
+//   TMA      : V tile (128 x BR, FP32) into a VST-deep ring; the Y tile
+//              (BR x KP, FP32) into a YST-deep ring; X (128 x KP, FP32) once.
+//   split    : the epilogue warps turn X and each Y tile into TF32 hi + lo parts in
+//              place (hi = round-to-nearest TF32, lo = x - hi, exact) and writes
+//              the transposed Y^T hi/lo tile that MMA2 reads K-major.  (An
+//              MN-major read of the Y tile returns zeros for TF32 on sm_100a.)
+//              Only FP32 factors travel from L2: 1 + KP/128 bytes per V byte.
+//   MMA1     : D (TMEM, 128 x BR, FP32) = Xl Yh^T + Xh Yl^T + Xh Yh^T
 //              (tcgen05.mma kind::tf32, A and B from shared memory, K-major).
 //   epilogue : R = V / D in FP32 registers (fdividef, as the reference),
-//              split R = Rh + Rl (Rh = TF32 round-to-nearest), written back to TMEM.
-//   MMA2     : Acc (TMEM, 128 x KP) += Rh Yh + Rh Yl + Rl Yh
-//              (kind::tf32, A = R from TMEM, B = the Y^T tile, K-major; an
-//              MN-major read of the Y tile returns zeros for TF32 on sm_100a,
-//              so the transposed copy of each factor is kept in HBM).
-//   end      : Acc -> the split's partial in global memory; k_muldiv (kernels_common.cu)
-//              sums the splits and applies X = X .* Xaux ./ colsum(Y).
+//              split R = Rh + Rl, written back to TMEM.
+//   MMA2     : Acc[tile] (TMEM, 128 x KP) = Rl Yh + Rh Yl + Rh Yh
+//              (kind::tf32, A = R from TMEM, B = Y^T from shared memory).
+//   epilogue : adds Acc[tile] into FP32 registers (per-tile accumulation keeps
+//              the tensor core's FP32 sums short), and at the end writes the
+//              split's partial; k_factor (kernels_common.cu) sums the splits
+//              and applies X = X .* Xaux ./ colsum(Y).
 //
 // Reference equivalent: get_H_BLM / get_W_BLN (src/NMF_routines.c:376-525,
 // 1014-1164): two cuBLAS SGEMMs around matrix_div_sub with WH in HBM.
 //
-// Warp roles (384 threads): warp 0 = V producer (TMA), warp 1 = MMA issuer and
-// TMEM owner, warp 2 = X/Y producer (TMA), warps 4-11 = epilogue (warp w
-// reads TMEM lanes 32*(w%4)..+31, column half (w-4)/4 of every tile).  V
-// stages are released as soon as the epilogue has read them; Y stages when
-// the second MMA that reads them has completed.
+// Warp roles (512 threads): warp 0 = V producer (TMA), warp 1 = MMA issuer and
+// TMEM owner, warp 2 = X/Y producer (TMA), warps 4-11 = R warps (warp w reads
+// TMEM lanes 32*(w%4)..+31, column half (w-4)/4 of every tile), warps 12-15 =
+// accumulator and split warps.
+// V stages are released as soon as the epilogue has read them, Y stages when
+// MMA1 has completed; a Y^T stage is rewritten only after the MMA2 that read
+// it has completed.
 // Every mbarrier wait is bounded (1 s of %globaltimer); on expiry the kernel
 // records an error word that the host turns into NMFB_ETIMEOUT.
 // No TMA multicast is used anywhere.
@@ -40,16 +46,15 @@ using nmfb::ConvState;
 namespace {
 
 constexpr int BO = 128;          // output rows per CTA = TMEM lanes
-constexpr int NTHREADS = 384;
+constexpr int NTHREADS = 512;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int SMEM_LIMIT = 232448; // max dynamic shared memory per block on sm_100
 constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;
 
 struct FusedMaps {
-    CUtensorMap v;
-    CUtensorMap xh, xl;  // updated factor, box rows = BO
-    CUtensorMap yh, yl;  // other factor, box rows = BR
-    CUtensorMap yth, ytl;  // other factor transposed (KP x rows), box = 32 x KP
+    CUtensorMap v;       // V, box [128 x BR] (H side, no swizzle) or [32 x 128] (W side, 128B swizzle)
+    CUtensorMap x;       // factor being updated (FP32, rows x KP), box rows = BO
+    CUtensorMap y;       // the other factor (FP32, rows x KP), box rows = BR
 };
 
 struct FusedArgs {
@@ -102,6 +107,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+// L2 eviction policies for TMA loads: the streamed V evict-first, the small
+// factor operands (re-read by every output block) evict-last.
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 // Bounded wait: false on timeout or when another role already aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort_flag,
                                           uint32_t *err, uint32_t code)
@@ -119,12 +140,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     return true;
 }
 
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y,
+                                            uint64_t policy)
 {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-            "r"(smem_u32(dst)),
-        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%3, %4}], [%2], %5;" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "l"(policy)
         : "memory");
 }
 
@@ -186,13 +208,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[32])
         : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[32])
-{
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-}
-
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[32])
 {
     asm volatile(
@@ -227,11 +242,11 @@ __device__ __forceinline__ void tmem_wait_ld_dep(uint32_t (&r)[32])
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+// Round to TF32 (10 mantissa bits), to nearest with ties away from zero, in
+// two integer operations; equal to cvt.rna.tf32.f32 for finite inputs.
 __device__ __forceinline__ float tf32_rna(float x)
 {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // Shared-memory matrix descriptor (tcgen05): start address, leading / stride
@@ -266,13 +281,13 @@ struct Geo {
     static constexpr int XBYTES = BO * KP * 4;
     static constexpr int YBYTES = BR * KP * 4;
     static constexpr int VBYTES = BO * BR * 4;
-    static constexpr int YSTAGE = 4 * YBYTES;              // Yh | Yl | YTh | YTl
-    static constexpr int YST = 3;                          // Y ring depth (L2-resident operand)
+    static constexpr int YSTAGE = 2 * YBYTES;              // Yh (TMA target, split in place) | Yl
+    static constexpr int YTSTAGE = 2 * YBYTES;             // YTh | YTl
+    static constexpr int YST = 3;
     static constexpr int FIXED = 1024 + 2 * XBYTES + 512;
-    static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YST * YSTAGE) / VBYTES;
+    static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YST * (YSTAGE + YTSTAGE)) / VBYTES;
     static constexpr int VST = VAVAIL > 6 ? 6 : VAVAIL;    // V ring depth (HBM stream)
-    static constexpr int SMEM = FIXED + YST * YSTAGE + VST * VBYTES;
-    static constexpr int HALF = KP / 2;                    // accumulator columns per epilogue warp
+    static constexpr int SMEM = FIXED + YST * (YSTAGE + YTSTAGE) + VST * VBYTES;
     static_assert(VST >= 2, "shared-memory ring too small");
 };
 
@@ -281,9 +296,57 @@ struct Geo {
 constexpr uint32_t ACC_COLS = 64;
 constexpr uint32_t DBUF0 = 128;
 
-// Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X/Y producer
-// (TMA), 3 = idle, 4..11 = epilogue.  Epilogue warp w reads TMEM lanes
-// 32*(w%4).. (hardware lane quadrant) and the column half (w-4)/4 of each tile.
+// Byte offset of element (row r, column c) in a K-major tile of G::CB-float
+// column blocks with 128B (CB = 32) or 64B (CB = 16) swizzle (the TMA layout).
+template <int KP>
+__device__ __forceinline__ uint32_t kmaj_off(uint32_t r, uint32_t c, uint32_t blk_bytes)
+{
+    using G = Geo<KP>;
+    uint32_t const b = c / G::CB, cc = c % G::CB;
+    uint32_t const chunk = cc >> 2;
+    uint32_t const sw = (G::CB == 32) ? (r & 7) : ((r >> 1) & 3);
+    return b * blk_bytes + r * G::ROWB + ((chunk ^ sw) << 4) + (cc & 3) * 4;
+}
+
+// Split rows [0, rows) of a K-major FP32 tile in place into TF32 hi (same
+// place) and lo (at `lo`, same layout); when `t_hi` is given, also write the
+// transpose (K-major over the rows, 128B swizzle: block of 32 rows = KP x 128 B).
+template <int KP>
+__device__ __forceinline__ void split_tile(unsigned char *hi, unsigned char *lo, unsigned char *t_hi,
+                                           unsigned char *t_lo, uint32_t rows, uint32_t blk_bytes, uint32_t tid,
+                                           uint32_t nthr)
+{
+    for (uint32_t q = tid; q < rows * (KP / 4); q += nthr) {
+        uint32_t const r = q / (KP / 4), c = (q % (KP / 4)) * 4;
+        {
+            uint32_t const off = kmaj_off<KP>(r, c, blk_bytes);
+            float4 const x = *reinterpret_cast<const float4 *>(hi + off);
+            float4 h, l;
+            h.x = tf32_rna(x.x); l.x = x.x - h.x;
+            h.y = tf32_rna(x.y); l.y = x.y - h.y;
+            h.z = tf32_rna(x.z); l.z = x.z - h.z;
+            h.w = tf32_rna(x.w); l.w = x.w - h.w;
+            *reinterpret_cast<float4 *>(hi + off) = h;
+            *reinterpret_cast<float4 *>(lo + off) = l;
+            if (t_hi) {
+                uint32_t const rb = r >> 5, rr = r & 31;
+                float hv[4] = {h.x, h.y, h.z, h.w}, lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    uint32_t const cc = c + i;
+                    uint32_t const toff = rb * (KP * 128) + cc * 128 + (((rr >> 2) ^ (cc & 7)) << 4) + (rr & 3) * 4;
+                    *reinterpret_cast<float *>(t_hi + toff) = hv[i];
+                    *reinterpret_cast<float *>(t_lo + toff) = lv[i];
+                }
+            }
+        }
+    }
+}
+
+// Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X and Y
+// producer (TMA), 3 = idle, 4..11 = R warps (V / D, feed MMA2), 12..15 =
+// accumulator warps (sum the per-tile MMA2 results in FP32 registers; split X
+// and, YST tiles ahead, each Y tile into TF32 hi/lo and its transpose).
 template <bool HSIDE, int KP, int NTERMS>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_fused_half(const __grid_constant__ FusedMaps maps, const FusedArgs args)
@@ -296,20 +359,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     extern __shared__ unsigned char smem_raw[];
     uint32_t const base_u32 = (smem_u32(smem_raw) + 1023u) & ~1023u;
     unsigned char *const base = smem_raw + (base_u32 - smem_u32(smem_raw));
-    unsigned char *const sXh = base;
+    unsigned char *const sXh = base;                                // TMA target, split in place
     unsigned char *const sXl = base + G::XBYTES;
-    unsigned char *const sY = base + 2 * G::XBYTES;                 // [YST][YSTAGE]
-    unsigned char *const sV = sY + G::YST * G::YSTAGE;              // [VST][VBYTES]
+    unsigned char *const sY = base + 2 * G::XBYTES;                 // [YST][Yh | Yl]
+    unsigned char *const sYT = sY + G::YST * G::YSTAGE;             // [YST][YTh | YTl]
+    unsigned char *const sV = sYT + G::YST * G::YTSTAGE;            // [VST][VBYTES]
     uint64_t *const bars = reinterpret_cast<uint64_t *>(sV + G::VST * G::VBYTES);
     uint64_t *const vfull = bars;                   // [VST]  TMA -> epilogue
     uint64_t *const vempty = vfull + G::VST;        // [VST]  epilogue -> V producer
-    uint64_t *const yfull = vempty + G::VST;        // [YST]  TMA -> MMA
-    uint64_t *const yempty = yfull + G::YST;        // [YST]  MMA2 commit -> Y producer
+    uint64_t *const yraw = vempty + G::VST;         // [YST]  TMA -> splitter
+    uint64_t *const yready = yraw + G::YST;         // [YST]  epilogue split -> MMA1 / MMA2
+    uint64_t *const yempty = yready + G::YST;       // [YST]  MMA1 commit -> Y producer
     uint64_t *const dfull = yempty + G::YST;        // [2]    MMA1 commit -> epilogue
     uint64_t *const rfull = dfull + 2;              // [2]    epilogue -> MMA2
-    uint64_t *const accrdy = rfull + 2;             // [2]    MMA2 commit -> epilogue
-    uint64_t *const xfull = accrdy + 2;             // [1]
-    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xfull + 1);
+    uint64_t *const accrdy = rfull + 2;             // [2]    MMA2 commit -> accumulator warps
+    uint64_t *const accfree = accrdy + 2;           // [2]    accumulator warps -> MMA2
+    uint64_t *const xraw = accfree + 2;             // [1]    TMA -> splitter
+    uint64_t *const xready = xraw + 1;              // [1]    epilogue split -> MMA1
+    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xready + 1);
     volatile uint32_t *const abort_flag = tmem_slot + 1;
 
     uint32_t const warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -320,6 +387,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint32_t const t_begin = split * args.tiles_per_split;
     uint32_t const t_end = min(T_all, t_begin + args.tiles_per_split);
     uint32_t const T = t_end > t_begin ? t_end - t_begin : 0;
+#ifdef NMFB_FUSED_DEBUG
+    // Per-tile event times of block 0 (ns since kernel start), 8 events x 64 tiles.
+    unsigned long long const ts0 = globaltimer();
+    unsigned long long *const dts = args.dbg ? reinterpret_cast<unsigned long long *>(args.dbg + 4 * BO * 64) : nullptr;
+#define DBG_TS(ev, t)                                                                              \
+    do {                                                                                           \
+        if (dts && blockIdx.x == 0 && (t) < 64) dts[(ev) * 64 + (t)] = globaltimer() - ts0;        \
+    } while (0)
+#else
+#define DBG_TS(ev, t) do { } while (0)
+#endif
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::VST; s++) {
@@ -327,15 +405,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&vempty[s], 8);
         }
         for (int s = 0; s < G::YST; s++) {
-            mbar_init(&yfull[s], 1);
+            mbar_init(&yraw[s], 1);
+            mbar_init(&yready[s], 4);
             mbar_init(&yempty[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&dfull[b], 1);
             mbar_init(&rfull[b], 8);
             mbar_init(&accrdy[b], 1);
+            mbar_init(&accfree[b], 4);
         }
-        mbar_init(xfull, 1);
+        mbar_init(xraw, 1);
+        mbar_init(xready, 4);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -350,11 +431,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tc_fence_after();
     uint32_t const tmem = *tmem_slot;
 
-    if (T == 0 || warp == 3) {
+    if (T == 0) {
         // idle
     } else if (warp == 0) {
         // ------------------------------------------------------------ V producer
         if (lane == 0) {
+            uint64_t const pol = policy_evict_first();
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::VST;
                 if (t >= (uint32_t)G::VST &&
@@ -362,243 +444,262 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     break;
                 unsigned char *sv = sV + s * G::VBYTES;
                 int const r0 = (int)((t_begin + t) * BR);
+                DBG_TS(0, t);
                 mbar_expect_tx(&vfull[s], G::VBYTES);
                 if (HSIDE) {
-                    tma_load_2d(sv, &maps.v, &vfull[s], (int)o0, r0);          // V[r0:r0+BR][o0:o0+128]
+                    tma_load_2d(sv, &maps.v, &vfull[s], (int)o0, r0, pol);     // V[r0:r0+BR][o0:o0+128]
                 } else {
 #pragma unroll
                     for (int b = 0; b < BR / 32; b++)                          // V[o0:o0+128][r0+32b : +32]
-                        tma_load_2d(sv + b * (BO * 128), &maps.v, &vfull[s], r0 + 32 * b, (int)o0);
+                        tma_load_2d(sv + b * (BO * 128), &maps.v, &vfull[s], r0 + 32 * b, (int)o0, pol);
                 }
             }
         }
     } else if (warp == 2) {
         // ------------------------------------------------------------ X / Y producer
         if (lane == 0) {
-            mbar_expect_tx(xfull, 2 * G::XBYTES);
-            for (int b = 0; b < G::NB; b++) {
-                tma_load_2d(sXh + b * G::XBLK, &maps.xh, xfull, b * G::CB, (int)o0);
-                tma_load_2d(sXl + b * G::XBLK, &maps.xl, xfull, b * G::CB, (int)o0);
-            }
+            uint64_t const pol = policy_evict_last();
+            mbar_expect_tx(xraw, G::XBYTES);
+            for (int b = 0; b < G::NB; b++) tma_load_2d(sXh + b * G::XBLK, &maps.x, xraw, b * G::CB, (int)o0, pol);
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::YST;
                 if (t >= (uint32_t)G::YST &&
                     !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 2u))
                     break;
                 unsigned char *syh = sY + s * G::YSTAGE;
-                unsigned char *syl = syh + G::YBYTES;
-                unsigned char *syth = syl + G::YBYTES;
-                unsigned char *sytl = syth + G::YBYTES;
                 int const r0 = (int)((t_begin + t) * BR);
-                mbar_expect_tx(&yfull[s], G::YSTAGE);
-                for (int b = 0; b < G::NB; b++) {
-                    tma_load_2d(syh + b * G::YBLK, &maps.yh, &yfull[s], b * G::CB, r0);
-                    tma_load_2d(syl + b * G::YBLK, &maps.yl, &yfull[s], b * G::CB, r0);
-                }
-#pragma unroll
-                for (int b = 0; b < BR / 32; b++) {                            // Y^T[0:KP][r0+32b : +32]
-                    tma_load_2d(syth + b * G::YTBLK, &maps.yth, &yfull[s], r0 + 32 * b, 0);
-                    tma_load_2d(sytl + b * G::YTBLK, &maps.ytl, &yfull[s], r0 + 32 * b, 0);
-                }
+                DBG_TS(1, t);
+                mbar_expect_tx(&yraw[s], G::YBYTES);
+                for (int b = 0; b < G::NB; b++) tma_load_2d(syh + b * G::YBLK, &maps.y, &yraw[s], b * G::CB, r0, pol);
             }
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
+        // Order: MMA1(0), MMA1(1); then for every tile t: MMA2(t) (after the R
+        // warps' R(t) and after the accumulator warps freed Acc[t % 2]) and
+        // MMA1(t+2) (after the accumulator warps split Y(t+2)).
         if (lane == 0) {
             constexpr uint32_t IDESC1 = idesc_tf32(BO, BR, 0);
             constexpr uint32_t IDESC2 = idesc_tf32(BO, KP, 0);
-            uint32_t const xh = smem_u32(sXh), xl = smem_u32(sXl);
-            bool ok = mbar_wait(xfull, 0, abort_flag, args.err, 3u);
-            tc_fence_after();
-            // Two issue queues: MMA1 of tile n1 (needs its Y stage and a free D
-            // buffer, i.e. MMA2 of tile n1-2 already issued) and MMA2 of tile n2
-            // (needs the epilogue's R of that tile).  Whichever is ready goes
-            // first, so a late Y stage never holds back the MMA2 that frees a stage.
-            uint32_t n1 = 0, n2 = 0;
-            unsigned long long last = globaltimer();
-            while (ok && n2 < T) {
-                bool progressed = false;
-                if (n1 < T && n1 <= n2 + 1) {
-                    uint32_t const s = n1 % G::YST, b = n1 & 1;
-                    if (mbar_try_wait(&yfull[s], (n1 / G::YST) & 1)) {
-                        tc_fence_after();
-                        uint32_t const yh = smem_u32(sY + s * G::YSTAGE);
-                        uint32_t const yl = yh + G::YBYTES;
-                        uint32_t const dcol = tmem + DBUF0 + b * 2 * BR;
-                        // MMA1: D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
-                        uint32_t acc = 0;
+            // Shared-memory descriptors are built once; a k-step or stage offset is
+            // added to the start-address field (16-byte units, no carry out of it:
+            // every operand lies below 256 KB).
+            uint64_t const dXh = smem_desc(smem_u32(sXh), 16, 8 * G::ROWB, G::LAYOUT);
+            uint64_t const dXl = smem_desc(smem_u32(sXl), 16, 8 * G::ROWB, G::LAYOUT);
+            uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
+            uint64_t const dYT0 = smem_desc(smem_u32(sYT), 16, 1024, 2u);
+            auto issue_mma1 = [&](uint32_t t1) {
+                uint32_t const s = t1 % G::YST, b = t1 & 1;
+                uint64_t const dYh = dY0 + ((s * G::YSTAGE) >> 4);
+                uint64_t const dYl = dYh + (G::YBYTES >> 4);
+                uint32_t const dcol = tmem + DBUF0 + b * 2 * BR;
+                // D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
 #pragma unroll
-                        for (int tt = 0; tt < NTERMS; tt++) {
-                            int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
-                            uint32_t const xa = (term == 2) ? xl : xh;
-                            uint32_t const yb = (term == 1) ? yl : yh;
+                for (int tt = 0; tt < NTERMS; tt++) {
+                    int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
+                    uint64_t const xa = (term == 2) ? dXl : dXh;
+                    uint64_t const yb = (term == 1) ? dYl : dYh;
 #pragma unroll
-                            for (int ks = 0; ks < KP / 8; ks++) {
-                                int const blk = ks / (G::CB / 8), within = (ks % (G::CB / 8)) * 32;
-                                uint64_t const ad = smem_desc(xa + blk * G::XBLK + within, 16, 8 * G::ROWB, G::LAYOUT);
-                                uint64_t const bd = smem_desc(yb + blk * G::YBLK + within, 16, 8 * G::ROWB, G::LAYOUT);
-                                mma_ss(dcol, ad, bd, IDESC1, acc);
-                                acc = 1;
-                            }
-                        }
-                        tc_commit(&dfull[b]);
-                        n1++;
-                        progressed = true;
+                    for (int ks = 0; ks < KP / 8; ks++) {
+                        constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
+                        uint32_t const oa = ((ks / KPB) * G::XBLK + (ks % KPB) * 32) >> 4;
+                        uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
+                        mma_ss(dcol, xa + oa, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
                     }
                 }
-                if (n2 < n1) {
-                    uint32_t const sp = n2 % G::YST, bp = n2 & 1;
-                    if (mbar_try_wait(&rfull[bp], (n2 >> 1) & 1)) {
-                        tc_fence_after();
-                        uint32_t const yth = smem_u32(sY + sp * G::YSTAGE + 2 * G::YBYTES);
-                        uint32_t const ytl = yth + G::YBYTES;
-                        uint32_t const rh = tmem + DBUF0 + bp * 2 * BR;
-                        uint32_t const rl = rh + BR;
-                        // MMA2: Acc[bp] = Rl Yh + Rh Yl + Rh Yh for this tile only; B = Y^T
-                        // (KP rows, K-major), K = BR reduction rows in steps of 8.  Tiles
-                        // are summed by the epilogue in FP32 registers.
-                        uint32_t acc = 0;
+                tc_commit(&dfull[b]);
+                tc_commit(&yempty[s]);
+                DBG_TS(2, t1);
+            };
+            bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u);
+            for (uint32_t t1 = 0; ok && t1 < 2 && t1 < T; t1++) {
+                ok = mbar_wait(&yready[t1 % G::YST], (t1 / G::YST) & 1, abort_flag, args.err, 4u);
+                if (!ok) break;
+                tc_fence_after();
+                issue_mma1(t1);
+            }
+            for (uint32_t t = 0; ok && t < T; t++) {
+                uint32_t const sp = t % G::YST, bp = t & 1;
+                if (!mbar_wait(&rfull[bp], (t >> 1) & 1, abort_flag, args.err, 5u)) break;
+                if (t >= 2 && !mbar_wait(&accfree[bp], ((t >> 1) - 1) & 1, abort_flag, args.err, 9u)) break;
+                tc_fence_after();
+                uint64_t const dYTh = dYT0 + ((sp * G::YTSTAGE) >> 4);
+                uint64_t const dYTl = dYTh + (G::YBYTES >> 4);
+                uint32_t const rh = tmem + DBUF0 + bp * 2 * BR;
+                uint32_t const rl = rh + BR;
+                uint32_t const dacc = tmem + bp * ACC_COLS;
+                // MMA2: Acc[bp] = Rl Yh + Rh Yl + Rh Yh for this tile only; B = Y^T
+                // (KP rows, K-major), K = BR reduction rows in steps of 8.
 #pragma unroll
-                        for (int tt = 0; tt < NTERMS; tt++) {
-                            int const term = NTERMS - 1 - tt;
-                            uint32_t const ra = (term == 2) ? rl : rh;
-                            uint32_t const yb = (term == 1) ? ytl : yth;
+                for (int tt = 0; tt < NTERMS; tt++) {
+                    int const term = NTERMS - 1 - tt;
+                    uint32_t const ra = (term == 2) ? rl : rh;
+                    uint64_t const yb = (term == 1) ? dYTl : dYTh;
 #pragma unroll
-                            for (int ks = 0; ks < BR / 8; ks++) {
-                                uint64_t const bd = smem_desc(yb + (ks / 4) * G::YTBLK + (ks % 4) * 32, 16, 1024, 2u);
-                                mma_ts(tmem + bp * ACC_COLS, ra + ks * 8, bd, IDESC2, acc);
-                                acc = 1;
-                            }
-                        }
-                        tc_commit(&yempty[sp]);
-                        tc_commit(&accrdy[bp]);
-                        n2++;
-                        progressed = true;
+                    for (int ks = 0; ks < BR / 8; ks++) {
+                        uint32_t const ob = ((ks / 4) * G::YTBLK + (ks % 4) * 32) >> 4;
+                        mma_ts(dacc, ra + ks * 8, yb + ob, IDESC2, (tt > 0 || ks > 0) ? 1u : 0u);
                     }
                 }
-                if (progressed) {
-                    last = globaltimer();
-                } else if (*abort_flag) {
-                    ok = false;
-                } else if (globaltimer() - last > WAIT_LIMIT_NS) {
-                    *abort_flag = 1;
-                    atomicExch(args.err, 4u);
-                    ok = false;
+                tc_commit(&accrdy[bp]);
+                DBG_TS(3, t);
+                uint32_t const t1 = t + 2;
+                if (t1 < T) {
+                    if (!mbar_wait(&yready[t1 % G::YST], (t1 / G::YST) & 1, abort_flag, args.err, 4u)) break;
+                    tc_fence_after();
+                    issue_mma1(t1);
                 }
             }
         }
-    } else {
-        // ------------------------------------------------------------ epilogue
+    } else if (warp >= 4 && warp < 12) {
+        // ------------------------------------------------------------ R warps
         uint32_t const quad = warp & 3;
         uint32_t const half = (warp - 4) >> 2;         // 0 or 1
         uint32_t const row = quad * 32 + lane;        // TMEM lane = output row within the block
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
-        float sum[G::HALF];
+        for (uint32_t t = 0; t < T; t++) {
+            uint32_t const s = t % G::VST, b = t & 1;
+            if (warp == 4 && lane == 0) DBG_TS(4, t);
+            if (!mbar_wait(&dfull[b], (t >> 1) & 1, abort_flag, args.err, 6u)) break;
+            if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) break;
+            tc_fence_after();
+            if (warp == 4 && lane == 0) DBG_TS(5, t);
+            const unsigned char *sv = sV + s * G::VBYTES;
+            uint32_t const dcol = DBUF0 + b * 2 * BR + half * QW;
+            uint32_t d[32];   // D, then the TF32 hi part of R
+            uint32_t v[32];   // V, then the lo part of R
+            if (QW == 32)
+                tmem_ld32(lane_addr + dcol, d);
+            else
+                tmem_ld16(lane_addr + dcol, d);
+            if (HSIDE) {
+                // V tile [BR rows][128 cols], row-major; this thread's column = row.
+                const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
 #pragma unroll
-        for (int c = 0; c < G::HALF; c++) sum[c] = 0.0f;
-        bool ok = true;
-        for (uint32_t t = 0; t <= T && ok; t++) {
-            if (t < T) {
-                uint32_t const s = t % G::VST, b = t & 1;
-                if (!mbar_wait(&dfull[b], (t >> 1) & 1, abort_flag, args.err, 6u)) { ok = false; break; }
-                if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) { ok = false; break; }
-                tc_fence_after();
-                const unsigned char *sv = sV + s * G::VBYTES;
-                uint32_t const dcol = DBUF0 + b * 2 * BR + half * QW;
-                uint32_t d[32];
-                if (QW == 32)
-                    tmem_ld32(lane_addr + dcol, d);
-                else
-                    tmem_ld16(lane_addr + dcol, d);
-                float v[32];
-                if (HSIDE) {
-                    // V tile [BR rows][128 cols], row-major; this thread's column = row.
-                    const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
+                for (int c = 0; c < QW; c++) v[c] = __float_as_uint(vs[c * BO]);
+            } else {
+                // V box `half` (BR == 64) or half a box (BR == 32): [128 rows][32 floats], 128B swizzle.
+                int const qb = (BR == 64) ? half : 0;
+                int const c0 = (BR == 64) ? 0 : half * 4;   // 16-byte chunk offset
+                const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
 #pragma unroll
-                    for (int c = 0; c < QW; c++) v[c] = vs[c * BO];
-                } else {
-                    // V box `half` (BR == 64) or half a box (BR == 32): [128 rows][32 floats], 128B swizzle.
-                    int const qb = (BR == 64) ? half : 0;
-                    int const c0 = (BR == 64) ? 0 : half * 4;   // 16-byte chunk offset
-                    const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
-#pragma unroll
-                    for (int c = 0; c < 32 / 4; c++) {
-                        if (c >= QW / 4) break;
-                        float4 const x = *reinterpret_cast<const float4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
-                        v[4 * c + 0] = x.x;
-                        v[4 * c + 1] = x.y;
-                        v[4 * c + 2] = x.z;
-                        v[4 * c + 3] = x.w;
-                    }
+                for (int c = 0; c < QW / 4; c++) {
+                    uint4 const x = *reinterpret_cast<const uint4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
+                    v[4 * c + 0] = x.x;
+                    v[4 * c + 1] = x.y;
+                    v[4 * c + 2] = x.z;
+                    v[4 * c + 3] = x.w;
                 }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
-                tmem_wait_ld_dep(d);
-                uint32_t hi[32], lo[32];
-#pragma unroll
-                for (int c = 0; c < QW; c++) {
-                    float const r = (v[c] == 0.0f) ? 0.0f : __fdividef(v[c], __uint_as_float(d[c]));
-                    float const h = tf32_rna(r);
-                    hi[c] = __float_as_uint(h);
-                    lo[c] = __float_as_uint(r - h);
-                }
-#ifdef NMFB_FUSED_DEBUG
-                if (args.dbg && blockIdx.x == 0 && t == 0)
-                    for (int c = 0; c < QW; c++) {
-                        args.dbg[row * 64 + half * QW + c] = __uint_as_float(d[c]);
-                        args.dbg[BO * 64 + row * 64 + half * QW + c] = v[c];
-                        args.dbg[2 * BO * 64 + row * 64 + half * QW + c] = __uint_as_float(hi[c]);
-                    }
-#endif
-                if (QW == 32) {
-                    tmem_st32(lane_addr + dcol, hi);
-                    if (NTERMS == 3) tmem_st32(lane_addr + dcol + BR, lo);
-                } else {
-                    tmem_st16(lane_addr + dcol, hi);
-                    if (NTERMS == 3) tmem_st16(lane_addr + dcol + BR, lo);
-                }
-                tmem_wait_st();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&rfull[b]);
             }
-            if (t >= 1) {
-                // Add the previous tile's accumulator (TMEM) into the FP32 registers.
-                uint32_t const tp = t - 1, bp = tp & 1;
-                if (!mbar_wait(&accrdy[bp], (tp >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
-                tc_fence_after();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
+            tmem_wait_ld_dep(d);
+#pragma unroll
+            for (int c = 0; c < QW; c++) {
+                float const vv = __uint_as_float(v[c]);
+                float const r = (vv == 0.0f) ? 0.0f : __fdividef(vv, __uint_as_float(d[c]));
+                float const h = tf32_rna(r);
+#ifdef NMFB_FUSED_DEBUG
+                if (args.dbg && blockIdx.x == 0 && t == 0) {
+                    args.dbg[row * 64 + half * QW + c] = __uint_as_float(d[c]);
+                    args.dbg[BO * 64 + row * 64 + half * QW + c] = vv;
+                    args.dbg[2 * BO * 64 + row * 64 + half * QW + c] = h;
+                }
+#endif
+                d[c] = __float_as_uint(h);
+                v[c] = __float_as_uint(r - h);
+            }
+            if (QW == 32) {
+                tmem_st32(lane_addr + dcol, d);
+                if (NTERMS == 3) tmem_st32(lane_addr + dcol + BR, v);
+            } else {
+                tmem_st16(lane_addr + dcol, d);
+                if (NTERMS == 3) tmem_st16(lane_addr + dcol + BR, v);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&rfull[b]);
+            if (warp == 4 && lane == 0) DBG_TS(6, t);
+#ifdef NMFB_FUSED_DEBUG
+            if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[512 + (warp - 4) * 64 + t] = globaltimer() - ts0;
+#endif
+        }
+    } else if (warp >= 12) {
+        // ------------------------------------------------------------ accumulator warps
+        // Warp 12+q owns TMEM lanes 32q..32q+31: sums the per-tile Acc into FP32
+        // registers, and (all four together) splits X and the Y tiles.
+        uint32_t const quad = warp & 3;
+        uint32_t const row = quad * 32 + lane;
+        uint32_t const lane_addr = tmem + ((quad * 32) << 16);
+        uint32_t const atid = (warp - 12) * 32 + lane;  // 0..127, for the cooperative splits
+        float sum[KP];
+#pragma unroll
+        for (int c = 0; c < KP; c++) sum[c] = 0.0f;
+        // Split Y(ty) (already in shared memory) into TF32 hi/lo and its transpose.
+        auto split_y = [&](uint32_t ty) -> bool {
+            uint32_t const s = ty % G::YST;
+            if (!mbar_wait(&yraw[s], (ty / G::YST) & 1, abort_flag, args.err, 11u)) return false;
+            unsigned char *syh = sY + s * G::YSTAGE;
+            unsigned char *syth = sYT + s * G::YTSTAGE;
+            split_tile<KP>(syh, syh + G::YBYTES, syth, syth + G::YBYTES, BR, G::YBLK, atid, 128);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&yready[s]);
+            return true;
+        };
+        bool ok = mbar_wait(xraw, 0, abort_flag, args.err, 10u);
+        if (ok) {
+            split_tile<KP>(sXh, sXl, nullptr, nullptr, BO, G::XBLK, atid, 128);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(xready);
+        }
+        for (uint32_t ty = 0; ok && ty < (uint32_t)G::YST && ty < T; ty++) ok = split_y(ty);
+        for (uint32_t t = 0; ok && t < T; t++) {
+            uint32_t const bp = t & 1;
+            if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
+            tc_fence_after();
+#pragma unroll
+            for (int c0 = 0; c0 < KP; c0 += 32) {
                 uint32_t a[32];
-                if (G::HALF == 32)
-                    tmem_ld32(lane_addr + bp * ACC_COLS + half * G::HALF, a);
-                else if (G::HALF == 16)
-                    tmem_ld16(lane_addr + bp * ACC_COLS + half * G::HALF, a);
+                if (KP - c0 >= 32)
+                    tmem_ld32(lane_addr + bp * ACC_COLS + c0, a);
                 else
-                    tmem_ld8(lane_addr + bp * ACC_COLS + half * G::HALF, a);
+                    tmem_ld16(lane_addr + bp * ACC_COLS + c0, a);
                 tmem_wait_ld_dep(a);
 #pragma unroll
-                for (int c = 0; c < G::HALF; c++) sum[c] += __uint_as_float(a[c]);
+                for (int c = 0; c < 32 && c0 + c < KP; c++) sum[c0 + c] += __uint_as_float(a[c]);
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accfree[bp]);
+            if (warp == 12 && lane == 0) DBG_TS(7, t);
+            // MMA2(t) has completed, so its Y^T stage (t % YST) is free: prepare Y(t + YST).
+            if (t + G::YST < T && !split_y(t + G::YST)) { ok = false; break; }
+#ifdef NMFB_FUSED_DEBUG
+            if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[1024 + (warp - 12) * 64 + t] = globaltimer() - ts0;
+#endif
         }
         if (ok) {
             uint32_t const o = o0 + row;
 #ifdef NMFB_FUSED_DEBUG
             if (args.dbg && blockIdx.x == 0)
-                for (int c = 0; c < G::HALF; c++) args.dbg[3 * BO * 64 + row * KP + half * G::HALF + c] = sum[c];
+                for (int c = 0; c < KP; c++) args.dbg[3 * BO * 64 + row * KP + c] = sum[c];
 #endif
             if (o < args.O) {
-                float *dst = args.part + ((size_t)split * args.O + o) * KP + half * G::HALF;
+                float *dst = args.part + ((size_t)split * args.O + o) * KP;
 #pragma unroll
-                for (int c = 0; c < G::HALF; c += 4)
+                for (int c = 0; c < KP; c += 4)
                     *reinterpret_cast<float4 *>(dst + c) = make_float4(sum[c], sum[c + 1], sum[c + 2], sum[c + 3]);
             }
         }
     }
-    if (T == 0 && warp >= 4) {
+    if (T == 0 && warp >= 12) {
         uint32_t const o = o0 + (warp & 3) * 32 + lane;
-        uint32_t const half = (warp - 4) >> 2;
         if (o < args.O) {
-            float *dst = args.part + ((size_t)split * args.O + o) * KP + half * G::HALF;
-            for (int c = 0; c < G::HALF; c++) dst[c] = 0.0f;
+            float *dst = args.part + ((size_t)split * args.O + o) * KP;
+            for (int c = 0; c < KP; c++) dst[c] = 0.0f;
         }
     }
     tc_fence_before();
@@ -715,8 +816,7 @@ int fused_half(nmfb_ctx *ctx, bool is_H, int adjust)
     if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
     int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH) : dispatch<false>(ctx, plan->mapsW);
     if (nsplit < 0) return nsplit;
-    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust,
-                     is_H ? &ctx->sH : &ctx->sW);
+    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust);
     if (rc) return rc;
     return nmfb_prof_end(ctx, whole);
 }
@@ -749,32 +849,23 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused error word: %s", cudaGetErrorString(e));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
 #ifdef NMFB_FUSED_DEBUG
-    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (3 * BO * 64 + BO * 64) * sizeof(float)));
-    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (3 * BO * 64 + BO * 64) * sizeof(float), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (4 * BO * 64 + 4096) * sizeof(float)));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (4 * BO * 64 + 4096) * sizeof(float), ctx->stream));
 #endif
     uint32_t const cb = (kp == 16) ? 16 : 32;
     CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
     uint64_t const vrow = ctx->ldv * sizeof(float), frow = (uint64_t)kp * sizeof(float);
     uint32_t const br = (kp >= 64) ? 32 : 64;
-    const nmfb::Split &W = ctx->sW, &H = ctx->sH;
     // update_H: X = H (rows m), Y = W (rows n); V tile [br rows of V][128 cols].
     FusedMaps &mh = plan->mapsH;
     if ((rc = encode_2d(ctx, &mh.v, ctx->dV, ctx->m, ctx->n, vrow, BO, br, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
-    if ((rc = encode_2d(ctx, &mh.xh, H.hi, kp, ctx->m, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.xl, H.lo, kp, ctx->m, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.yh, W.hi, kp, ctx->n, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.yl, W.lo, kp, ctx->n, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.yth, W.hiT, ctx->n, kp, W.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode_2d(ctx, &mh.ytl, W.loT, ctx->n, kp, W.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode_2d(ctx, &mh.x, ctx->dH, kp, ctx->m, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.y, ctx->dW, kp, ctx->n, frow, cb, br, fsw))) return rc;
     // update_W: X = W (rows n), Y = H (rows m); V tile [128 rows][32 cols] x (br/32), 128B swizzle.
     FusedMaps &mw = plan->mapsW;
     if ((rc = encode_2d(ctx, &mw.v, ctx->dV, ctx->m, ctx->n, vrow, 32, BO, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode_2d(ctx, &mw.xh, W.hi, kp, ctx->n, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.xl, W.lo, kp, ctx->n, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.yh, H.hi, kp, ctx->m, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.yl, H.lo, kp, ctx->m, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.yth, H.hiT, ctx->m, kp, H.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode_2d(ctx, &mw.ytl, H.loT, ctx->m, kp, H.ldT * 4, 32, kp, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode_2d(ctx, &mw.x, ctx->dW, kp, ctx->n, frow, cb, BO, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.y, ctx->dH, kp, ctx->m, frow, cb, br, fsw))) return rc;
     return NMFB_OK;
 }
 
@@ -805,7 +896,7 @@ int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
 extern "C" int nmfb_debug_dump(nmfb_ctx *ctx, float *host)
 {
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
-    NMFB_CUDA_TRY(ctx, cudaMemcpy(host, plan->dDbg, (3 * BO * 64 + BO * 64) * sizeof(float), cudaMemcpyDeviceToHost));
+    NMFB_CUDA_TRY(ctx, cudaMemcpy(host, plan->dDbg, (4 * BO * 64 + 4096) * sizeof(float), cudaMemcpyDeviceToHost));
     return NMFB_OK;
 }
 #endif

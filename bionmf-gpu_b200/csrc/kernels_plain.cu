@@ -187,7 +187,7 @@ int plain_half(nmfb_ctx *ctx, bool is_H, int adjust)
     NMFB_LAUNCH_CHECK(ctx);
     if ((rc = nmfb_prof_end(ctx, main))) return rc;
     // 5. X = X .* Xaux ./ acc  (+ EPS adjust on test iterations)
-    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, p.nsplit, (size_t)xrows * ctx->kp, acc, adjust, nullptr);
+    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, p.nsplit, (size_t)xrows * ctx->kp, acc, adjust);
     if (rc) return rc;
     return nmfb_prof_end(ctx, whole);
 }

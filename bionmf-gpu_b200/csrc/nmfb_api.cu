@@ -44,10 +44,9 @@ int dev_alloc(nmfb_ctx *ctx, T **p, size_t items, const char *what)
 
 void free_all(nmfb_ctx *ctx)
 {
-    void *bufs[] = {ctx->dV,   ctx->dW,    ctx->dH,     ctx->dAccW,  ctx->dAccH,  ctx->dWH,    ctx->dPart,
-                    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->sW.hi, ctx->sW.lo, ctx->sW.hiT,
-                    ctx->sW.loT, ctx->sH.hi, ctx->sH.lo, ctx->sH.hiT, ctx->sH.loT, ctx->dLabels, ctx->dFirst,
-                    ctx->dLastRep, ctx->dState};
+    void *bufs[] = {ctx->dV,       ctx->dW,       ctx->dH,    ctx->dAccW,       ctx->dAccH,   ctx->dWH,
+                    ctx->dPart,    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->dLabels,
+                    ctx->dFirst,   ctx->dLastRep, ctx->dState};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->hState) cudaFreeHost(ctx->hState);
@@ -91,14 +90,6 @@ int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, 
     cudaFreeHost(stage);
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "download: %s", cudaGetErrorString(e));
     return NMFB_OK;
-}
-
-int refresh_splits(nmfb_ctx *ctx)
-{
-    if (!ctx->sW.hi) return NMFB_OK;
-    int rc = nmfb_split_tf32(ctx, ctx->dW, ctx->n, &ctx->sW);
-    if (rc) return rc;
-    return nmfb_split_tf32(ctx, ctx->dH, ctx->m, &ctx->sH);
 }
 
 int do_update_H(nmfb_ctx *ctx, int adjust)
@@ -223,21 +214,6 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
     }
     if (ctx->kp > 64)
         return nmfb_fail(ctx, NMFB_EINVAL, "the fused arms support ranks up to 64 (k=%u); use NMFB_ARM_PLAIN", ctx->k);
-    if (!ctx->sW.hi) {
-        size_t const kp = ctx->kp;
-        struct { nmfb::Split *s; uint32_t rows; const char *name; } f[2] = {{&ctx->sW, ctx->n, "W"}, {&ctx->sH, ctx->m, "H"}};
-        for (auto &x : f) {
-            x.s->ldT = ((size_t)x.rows + 31) / 32 * 32;
-            if ((rc = dev_alloc(ctx, &x.s->hi, (size_t)x.rows * kp, x.name))) return rc;
-            if ((rc = dev_alloc(ctx, &x.s->lo, (size_t)x.rows * kp, x.name))) return rc;
-            if ((rc = dev_alloc(ctx, &x.s->hiT, kp * x.s->ldT, x.name))) return rc;
-            if ((rc = dev_alloc(ctx, &x.s->loT, kp * x.s->ldT, x.name))) return rc;
-            NMFB_CUDA_TRY(ctx, cudaMemsetAsync(x.s->hiT, 0, kp * x.s->ldT * sizeof(float), ctx->stream));
-            NMFB_CUDA_TRY(ctx, cudaMemsetAsync(x.s->loT, 0, kp * x.s->ldT * sizeof(float), ctx->stream));
-        }
-    }
-    // W and H may have been changed by another arm: refresh their TF32 splits.
-    if ((rc = refresh_splits(ctx))) return rc;
     if ((rc = nmfb_fused_prepare(ctx))) return rc;
     ctx->arm = arm;
     return NMFB_OK;
@@ -312,7 +288,6 @@ int nmfb_set_WH(nmfb_ctx *ctx, const float *W, size_t ldw, const float *H, size_
     if (!W || !H || ldw < ctx->k || ldh < ctx->k) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_WH: bad arguments");
     if ((rc = upload_factor(ctx, ctx->dW, W, ctx->n, ctx->k, ldw))) return rc;
     if ((rc = upload_factor(ctx, ctx->dH, H, ctx->m, ctx->k, ldh))) return rc;
-    if ((rc = refresh_splits(ctx))) return rc;
     ctx->wh_set = 1;
     return NMFB_OK;
 }

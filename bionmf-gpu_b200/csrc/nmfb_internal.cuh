@@ -23,13 +23,6 @@ struct ConvState {
     uint32_t pad;
 };
 
-// TF32 hi/lo split of one factor for the tensor-core arms: row-major
-// (rows x kp) and transposed (kp x ldT, ldT = rows rounded up to 32).
-struct Split {
-    float *hi, *lo, *hiT, *loT;
-    size_t ldT;
-};
-
 }  // namespace nmfb
 
 struct nmfb_ctx {
@@ -51,8 +44,6 @@ struct nmfb_ctx {
     double *dObj;          // objective partials + results
     uint32_t *dObjTicket;
 
-    // tcgen05 arms: TF32 hi/lo splits of the factors (null for the plain arm).
-    nmfb::Split sW, sH;
     int sm_count;
     void *tmaps;           // fused-arm tensor maps (host copy), see kernels_fused.cu
 
@@ -103,13 +94,12 @@ extern "C" int nmfb_prof_end(nmfb_ctx *ctx, int cls);
 // ---- kernels_common.cu ----------------------------------------------------
 int nmfb_colsum(nmfb_ctx *ctx, const float *X, uint32_t rows, float *acc, int which);
 int nmfb_muldiv(nmfb_ctx *ctx, float *X, uint32_t rows, const float *part, uint32_t nsplit,
-                size_t split_stride, const float *acc, int adjust, const nmfb::Split *split);
+                size_t split_stride, const float *acc, int adjust);
 int nmfb_adjust_rows(nmfb_ctx *ctx, float *X, uint32_t rows);
 int nmfb_classify_and_test(nmfb_ctx *ctx, uint32_t niter_test_conv);
 int nmfb_classify_only(nmfb_ctx *ctx);
 int nmfb_reset_conv(nmfb_ctx *ctx, uint32_t stop_threshold);
 int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl);
-int nmfb_split_tf32(nmfb_ctx *ctx, float *X, uint32_t rows, const nmfb::Split *split);
 
 // ---- kernels_plain.cu -----------------------------------------------------
 int nmfb_plain_update_H(nmfb_ctx *ctx, int adjust);
