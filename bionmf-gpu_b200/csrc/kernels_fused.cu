@@ -14,7 +14,8 @@
 //              Only FP32 factors travel from L2: 1 + KP/128 bytes per V byte.
 //   MMA1     : D (TMEM, 128 x BR, FP32) = Xl Yh^T + Xh Yl^T + Xh Yh^T
 //              (tcgen05.mma kind::tf32, A and B from shared memory, K-major).
-//   epilogue : R = V / D in FP32 registers (fdividef, as the reference),
+//   epilogue : R = V / D in FP32 registers (V times an approximate reciprocal,
+//              <= 1.5 ulp; the reference uses fdividef),
 //              split R = Rh + Rl, written back to TMEM.
 //   MMA2     : Acc[tile] (TMEM, 128 x KP) = Rl Yh + Rh Yl + Rh Yh
 //              (kind::tf32, A = R from TMEM, B = Y^T from shared memory).
@@ -39,6 +40,7 @@
 #include "nmfb_internal.cuh"
 
 #include <cuda.h>
+#include <float.h>
 #include <cudaTypedefs.h>
 
 using nmfb::ConvState;
@@ -46,7 +48,6 @@ using nmfb::ConvState;
 namespace {
 
 constexpr int BO = 128;          // output rows per CTA = TMEM lanes
-constexpr int NTHREADS = 512;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int SMEM_LIMIT = 232448; // max dynamic shared memory per block on sm_100
 constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;
@@ -100,6 +101,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Non-blocking probe of a phase (mbarrier.test_wait never suspends the thread).
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity)
@@ -242,6 +257,14 @@ __device__ __forceinline__ void tmem_wait_ld_dep(uint32_t (&r)[32])
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+// 1/x with rcp.approx.ftz.f32 (PTX: at most 1 ulp of error over the full range).
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Round to TF32 (10 mantissa bits), to nearest with ties away from zero, in
 // two integer operations; equal to cvt.rna.tf32.f32 for finite inputs.
 __device__ __forceinline__ float tf32_rna(float x)
@@ -277,7 +300,8 @@ struct Geo {
     static constexpr uint32_t LAYOUT = (KP == 16) ? 4u : 2u;  // SW64 : SW128
     static constexpr int XBLK = BO * ROWB;                 // bytes of one X column block
     static constexpr int YBLK = BR * ROWB;                 // bytes of one Y column block
-    static constexpr int YTBLK = KP * 128;                 // bytes of one Y^T block (32 reduction rows)
+    static constexpr int YTBLK = KP * 128;                 // bytes of one Y^T part (32 reduction rows)
+    static constexpr int YTPAIR = 2 * YTBLK;               // Y^T hi part followed by its lo part
     static constexpr int XBYTES = BO * KP * 4;
     static constexpr int YBYTES = BR * KP * 4;
     static constexpr int VBYTES = BO * BR * 4;
@@ -289,12 +313,18 @@ struct Geo {
     static constexpr int VST = VAVAIL > 6 ? 6 : VAVAIL;    // V ring depth (HBM stream)
     static constexpr int SMEM = FIXED + YST * (YSTAGE + YTSTAGE) + VST * VBYTES;
     static_assert(VST >= 2, "shared-memory ring too small");
+    static constexpr int NR = (KP >= 64) ? 8 : 16;        // R warps
+    static constexpr int QW = BR / (NR / 4);               // tile columns per R warp
+    static constexpr int NTHR = (4 + NR + 4) * 32;
+    static constexpr uint32_t ACC = 2 * KP;                // TMEM columns of one per-tile accumulator
+    static constexpr uint32_t DB0 = 2 * ACC;               // first D buffer column
 };
 
-// TMEM columns: per-tile accumulators Acc[b] at b*64 (KP <= 64 columns each),
-// D[b] (later Rh[b]) at 128 + b*2*BR, Rl[b] at 128 + b*2*BR + BR.
-constexpr uint32_t ACC_COLS = 64;
-constexpr uint32_t DBUF0 = 128;
+// TMEM columns: per-tile accumulators Acc[b] at b*2KP (2KP columns: the Rh Y^T_hi
+// + Rl Y^T_hi sum and the Rh Y^T_lo part side by side), D[b] (later Rh[b]) at
+// 4KP + b*2*BR, Rl[b] at 4KP + b*2*BR + BR, b < NDB.  Three D buffers let MMA1
+// run three tiles ahead of the R warps (KP=32: 128 + 3*128 = 512 columns).
+constexpr uint32_t NDB = 3;
 
 // Byte offset of element (row r, column c) in a K-major tile of G::CB-float
 // column blocks with 128B (CB = 32) or 64B (CB = 16) swizzle (the TMA layout).
@@ -310,11 +340,12 @@ __device__ __forceinline__ uint32_t kmaj_off(uint32_t r, uint32_t c, uint32_t bl
 
 // Split rows [0, rows) of a K-major FP32 tile in place into TF32 hi (same
 // place) and lo (at `lo`, same layout); when `t_hi` is given, also write the
-// transpose (K-major over the rows, 128B swizzle: block of 32 rows = KP x 128 B).
+// transpose (K-major over the rows, 128B swizzle; for each block of 32 rows
+// the hi part, KP x 128 B, directly followed by the lo part, so that one MMA
+// with N = 2 KP reads both).
 template <int KP>
 __device__ __forceinline__ void split_tile(unsigned char *hi, unsigned char *lo, unsigned char *t_hi,
-                                           unsigned char *t_lo, uint32_t rows, uint32_t blk_bytes, uint32_t tid,
-                                           uint32_t nthr)
+                                           uint32_t rows, uint32_t blk_bytes, uint32_t tid, uint32_t nthr)
 {
     for (uint32_t q = tid; q < rows * (KP / 4); q += nthr) {
         uint32_t const r = q / (KP / 4), c = (q % (KP / 4)) * 4;
@@ -329,14 +360,15 @@ __device__ __forceinline__ void split_tile(unsigned char *hi, unsigned char *lo,
             *reinterpret_cast<float4 *>(hi + off) = h;
             *reinterpret_cast<float4 *>(lo + off) = l;
             if (t_hi) {
+                // Y^T: per block of 32 rows, the hi part (KP rows of 128 B) followed by the lo part.
                 uint32_t const rb = r >> 5, rr = r & 31;
                 float hv[4] = {h.x, h.y, h.z, h.w}, lv[4] = {l.x, l.y, l.z, l.w};
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     uint32_t const cc = c + i;
-                    uint32_t const toff = rb * (KP * 128) + cc * 128 + (((rr >> 2) ^ (cc & 7)) << 4) + (rr & 3) * 4;
+                    uint32_t const toff = rb * (2 * KP * 128) + cc * 128 + (((rr >> 2) ^ (cc & 7)) << 4) + (rr & 3) * 4;
                     *reinterpret_cast<float *>(t_hi + toff) = hv[i];
-                    *reinterpret_cast<float *>(t_lo + toff) = lv[i];
+                    *reinterpret_cast<float *>(t_hi + toff + KP * 128) = lv[i];
                 }
             }
         }
@@ -348,12 +380,15 @@ __device__ __forceinline__ void split_tile(unsigned char *hi, unsigned char *lo,
 // accumulator warps (sum the per-tile MMA2 results in FP32 registers; split X
 // and, YST tiles ahead, each Y tile into TF32 hi/lo and its transpose).
 template <bool HSIDE, int KP, int NTERMS>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     k_fused_half(const __grid_constant__ FusedMaps maps, const FusedArgs args)
 {
     using G = Geo<KP>;
     constexpr int BR = G::BR;
-    constexpr int QW = BR / 2;          // tile columns handled by one epilogue warp
+    constexpr int QW = G::QW;           // tile columns handled by one R warp
+    constexpr int NR = G::NR;
+    constexpr uint32_t ACC_COLS = G::ACC;
+    constexpr uint32_t DBUF0 = G::DB0;
     if (args.st && *(volatile const uint32_t *)&args.st->converged) return;
 
     extern __shared__ unsigned char smem_raw[];
@@ -370,9 +405,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint64_t *const yraw = vempty + G::VST;         // [YST]  TMA -> splitter
     uint64_t *const yready = yraw + G::YST;         // [YST]  epilogue split -> MMA1 / MMA2
     uint64_t *const yempty = yready + G::YST;       // [YST]  MMA1 commit -> Y producer
-    uint64_t *const dfull = yempty + G::YST;        // [2]    MMA1 commit -> epilogue
-    uint64_t *const rfull = dfull + 2;              // [2]    epilogue -> MMA2
-    uint64_t *const accrdy = rfull + 2;             // [2]    MMA2 commit -> accumulator warps
+    uint64_t *const dfull = yempty + G::YST;        // [NDB]  MMA1 commit -> R warps
+    uint64_t *const rfull = dfull + NDB;            // [NDB]  R warps -> MMA2
+    uint64_t *const accrdy = rfull + NDB;           // [2]    MMA2 commit -> accumulator warps
     uint64_t *const accfree = accrdy + 2;           // [2]    accumulator warps -> MMA2
     uint64_t *const xraw = accfree + 2;             // [1]    TMA -> splitter
     uint64_t *const xready = xraw + 1;              // [1]    epilogue split -> MMA1
@@ -395,23 +430,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     do {                                                                                           \
         if (dts && blockIdx.x == 0 && (t) < 64) dts[(ev) * 64 + (t)] = globaltimer() - ts0;        \
     } while (0)
+#define DBG_PH(ph, t)                                                                                 \
+    do {                                                                                              \
+        if (dts && blockIdx.x == 0 && warp == 5 && lane == 0 && (t) < 64)                             \
+            dts[1536 + (ph) * 64 + (t)] = clock64();                                                  \
+    } while (0)
 #else
 #define DBG_TS(ev, t) do { } while (0)
+#define DBG_PH(ph, t) do { } while (0)
 #endif
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::VST; s++) {
             mbar_init(&vfull[s], 1);
-            mbar_init(&vempty[s], 8);
+            mbar_init(&vempty[s], NR);
         }
         for (int s = 0; s < G::YST; s++) {
             mbar_init(&yraw[s], 1);
             mbar_init(&yready[s], 4);
             mbar_init(&yempty[s], 1);
         }
-        for (int b = 0; b < 2; b++) {
+        for (uint32_t b = 0; b < NDB; b++) {
             mbar_init(&dfull[b], 1);
-            mbar_init(&rfull[b], 8);
+            mbar_init(&rfull[b], NR);
+        }
+        for (int b = 0; b < 2; b++) {
             mbar_init(&accrdy[b], 1);
             mbar_init(&accfree[b], 4);
         }
@@ -475,12 +518,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
-        // Order: MMA1(0), MMA1(1); then for every tile t: MMA2(t) (after the R
-        // warps' R(t) and after the accumulator warps freed Acc[t % 2]) and
-        // MMA1(t+2) (after the accumulator warps split Y(t+2)).
+        // Two issue queues, polled without blocking (nanosleep back-off):
+        //   MMA2(n2): needs the R warps' R(n2) and, for n2 >= 2, the accumulator
+        //             warps to have read Acc[n2 % 2] of tile n2-2;
+        //   MMA1(n1): needs the split Y(n1) and a free D buffer (MMA2(n1-NDB)
+        //             issued, i.e. n1 < n2 + NDB).
         if (lane == 0) {
             constexpr uint32_t IDESC1 = idesc_tf32(BO, BR, 0);
             constexpr uint32_t IDESC2 = idesc_tf32(BO, KP, 0);
+            constexpr uint32_t IDESC2W = idesc_tf32(BO, 2 * KP, 0);
             // Shared-memory descriptors are built once; a k-step or stage offset is
             // added to the start-address field (16-byte units, no carry out of it:
             // every operand lies below 256 KB).
@@ -488,81 +534,94 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             uint64_t const dXl = smem_desc(smem_u32(sXl), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dYT0 = smem_desc(smem_u32(sYT), 16, 1024, 2u);
-            auto issue_mma1 = [&](uint32_t t1) {
-                uint32_t const s = t1 % G::YST, b = t1 & 1;
-                uint64_t const dYh = dY0 + ((s * G::YSTAGE) >> 4);
-                uint64_t const dYl = dYh + (G::YBYTES >> 4);
-                uint32_t const dcol = tmem + DBUF0 + b * 2 * BR;
-                // D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
-#pragma unroll
-                for (int tt = 0; tt < NTERMS; tt++) {
-                    int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
-                    uint64_t const xa = (term == 2) ? dXl : dXh;
-                    uint64_t const yb = (term == 1) ? dYl : dYh;
-#pragma unroll
-                    for (int ks = 0; ks < KP / 8; ks++) {
-                        constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
-                        uint32_t const oa = ((ks / KPB) * G::XBLK + (ks % KPB) * 32) >> 4;
-                        uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
-                        mma_ss(dcol, xa + oa, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
-                    }
-                }
-                tc_commit(&dfull[b]);
-                tc_commit(&yempty[s]);
-                DBG_TS(2, t1);
-            };
             bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u);
-            for (uint32_t t1 = 0; ok && t1 < 2 && t1 < T; t1++) {
-                ok = mbar_wait(&yready[t1 % G::YST], (t1 / G::YST) & 1, abort_flag, args.err, 4u);
-                if (!ok) break;
-                tc_fence_after();
-                issue_mma1(t1);
-            }
-            for (uint32_t t = 0; ok && t < T; t++) {
-                uint32_t const sp = t % G::YST, bp = t & 1;
-                if (!mbar_wait(&rfull[bp], (t >> 1) & 1, abort_flag, args.err, 5u)) break;
-                if (t >= 2 && !mbar_wait(&accfree[bp], ((t >> 1) - 1) & 1, abort_flag, args.err, 9u)) break;
-                tc_fence_after();
-                uint64_t const dYTh = dYT0 + ((sp * G::YTSTAGE) >> 4);
-                uint64_t const dYTl = dYTh + (G::YBYTES >> 4);
-                uint32_t const rh = tmem + DBUF0 + bp * 2 * BR;
-                uint32_t const rl = rh + BR;
-                uint32_t const dacc = tmem + bp * ACC_COLS;
-                // MMA2: Acc[bp] = Rl Yh + Rh Yl + Rh Yh for this tile only; B = Y^T
-                // (KP rows, K-major), K = BR reduction rows in steps of 8.
-#pragma unroll
-                for (int tt = 0; tt < NTERMS; tt++) {
-                    int const term = NTERMS - 1 - tt;
-                    uint32_t const ra = (term == 2) ? rl : rh;
-                    uint64_t const yb = (term == 1) ? dYTl : dYTh;
+            tc_fence_after();
+            uint32_t n1 = 0, n2 = 0;
+            unsigned long long last = globaltimer();
+            while (ok && n2 < T) {
+                bool progressed = false;
+                if (n2 < n1 && mbar_test(&rfull[n2 % NDB], (n2 / NDB) & 1) &&
+                    (n2 < 2 || mbar_test(&accfree[n2 & 1], ((n2 >> 1) - 1) & 1))) {
+                    tc_fence_after();
+                    uint32_t const sp = n2 % G::YST, bp = n2 & 1, db = n2 % NDB;
+                    uint64_t const dYT = dYT0 + ((sp * G::YTSTAGE) >> 4);
+                    uint32_t const rh = tmem + DBUF0 + db * 2 * BR;
+                    uint32_t const rl = rh + BR;
+                    uint32_t const dacc = tmem + bp * ACC_COLS;
+                    // MMA2 for this tile only, K = BR reduction rows in steps of 8:
+                    //   Acc[bp][0:2KP] (+)= Rh [Y^T_hi; Y^T_lo]   (one MMA, N = 2 KP)
+                    //   Acc[bp][0:KP]   += Rl Y^T_hi              (N = KP)
+                    // so Acc[0:KP] + Acc[KP:2KP] = Rh Yh + Rl Yh + Rh Yl (summed by the
+                    // accumulator warps in FP32 registers).
 #pragma unroll
                     for (int ks = 0; ks < BR / 8; ks++) {
-                        uint32_t const ob = ((ks / 4) * G::YTBLK + (ks % 4) * 32) >> 4;
-                        mma_ts(dacc, ra + ks * 8, yb + ob, IDESC2, (tt > 0 || ks > 0) ? 1u : 0u);
+                        uint32_t const ob = ((ks / 4) * G::YTPAIR + (ks % 4) * 32) >> 4;
+                        if (NTERMS == 3) {
+                            mma_ts(dacc, rh + ks * 8, dYT + ob, IDESC2W, ks > 0 ? 1u : 0u);
+                            mma_ts(dacc, rl + ks * 8, dYT + ob, IDESC2, 1u);
+                        } else {
+                            mma_ts(dacc, rh + ks * 8, dYT + ob, IDESC2, ks > 0 ? 1u : 0u);
+                        }
                     }
+                    tc_commit(&accrdy[bp]);
+                    DBG_TS(3, n2);
+                    n2++;
+                    progressed = true;
                 }
-                tc_commit(&accrdy[bp]);
-                DBG_TS(3, t);
-                uint32_t const t1 = t + 2;
-                if (t1 < T) {
-                    if (!mbar_wait(&yready[t1 % G::YST], (t1 / G::YST) & 1, abort_flag, args.err, 4u)) break;
+                if (n1 < T && n1 < n2 + NDB && mbar_test(&yready[n1 % G::YST], (n1 / G::YST) & 1)) {
                     tc_fence_after();
-                    issue_mma1(t1);
+                    uint32_t const s = n1 % G::YST, db = n1 % NDB;
+                    uint64_t const dYh = dY0 + ((s * G::YSTAGE) >> 4);
+                    uint64_t const dYl = dYh + (G::YBYTES >> 4);
+                    uint32_t const dcol = tmem + DBUF0 + db * 2 * BR;
+                    // MMA1: D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
+#pragma unroll
+                    for (int tt = 0; tt < NTERMS; tt++) {
+                        int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
+                        uint64_t const xa = (term == 2) ? dXl : dXh;
+                        uint64_t const yb = (term == 1) ? dYl : dYh;
+#pragma unroll
+                        for (int ks = 0; ks < KP / 8; ks++) {
+                            constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
+                            uint32_t const oa = ((ks / KPB) * G::XBLK + (ks % KPB) * 32) >> 4;
+                            uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
+                            mma_ss(dcol, xa + oa, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc_commit(&dfull[db]);
+                    tc_commit(&yempty[s]);
+                    DBG_TS(2, n1);
+                    n1++;
+                    progressed = true;
+                }
+                if (progressed) {
+                    last = globaltimer();
+                } else if (*abort_flag) {
+                    ok = false;
+                } else if (globaltimer() - last > WAIT_LIMIT_NS) {
+                    *abort_flag = 1;
+                    atomicExch(args.err, 4u);
+                    ok = false;
+                } else {
+                    __nanosleep(64);
                 }
             }
         }
-    } else if (warp >= 4 && warp < 12) {
+    } else if (warp >= 4 && warp < 4 + NR) {
         // ------------------------------------------------------------ R warps
         uint32_t const quad = warp & 3;
-        uint32_t const half = (warp - 4) >> 2;         // 0 or 1
+        uint32_t const half = (warp - 4) >> 2;         // column group of this warp
         uint32_t const row = quad * 32 + lane;        // TMEM lane = output row within the block
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
         for (uint32_t t = 0; t < T; t++) {
-            uint32_t const s = t % G::VST, b = t & 1;
+            uint32_t const s = t % G::VST, b = t % NDB;
             if (warp == 4 && lane == 0) DBG_TS(4, t);
-            if (!mbar_wait(&dfull[b], (t >> 1) & 1, abort_flag, args.err, 6u)) break;
+            DBG_PH(0, t);
+            if (!mbar_wait(&dfull[b], (t / NDB) & 1, abort_flag, args.err, 6u)) break;
+            DBG_PH(1, t);
             if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) break;
             tc_fence_after();
+            DBG_PH(2, t);
             if (warp == 4 && lane == 0) DBG_TS(5, t);
             const unsigned char *sv = sV + s * G::VBYTES;
             uint32_t const dcol = DBUF0 + b * 2 * BR + half * QW;
@@ -578,9 +637,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                 for (int c = 0; c < QW; c++) v[c] = __float_as_uint(vs[c * BO]);
             } else {
-                // V box `half` (BR == 64) or half a box (BR == 32): [128 rows][32 floats], 128B swizzle.
-                int const qb = (BR == 64) ? half : 0;
-                int const c0 = (BR == 64) ? 0 : half * 4;   // 16-byte chunk offset
+                // V boxes of [128 rows][32 floats], 128B swizzle; this warp's QW columns.
+                int const qb = (half * QW) / 32;
+                int const c0 = ((half * QW) % 32) / 4;      // 16-byte chunk offset within the box
                 const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
 #pragma unroll
                 for (int c = 0; c < QW / 4; c++) {
@@ -591,13 +650,27 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     v[4 * c + 3] = x.w;
                 }
             }
+#ifdef NMFB_FUSED_DEBUG
+            {   // debug timing only: consume the loaded V values before the next phase mark
+                uint32_t x = 0;
+#pragma unroll
+                for (int c = 0; c < QW; c++) x ^= v[c];
+                asm volatile("" ::"r"(x));
+                if (x == 0x7fffffffu && dts) dts[0] = x;
+            }
+#endif
             __syncwarp();
             if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
+            DBG_PH(3, t);
             tmem_wait_ld_dep(d);
+            DBG_PH(4, t);
 #pragma unroll
             for (int c = 0; c < QW; c++) {
+                // R = V / WH as V * (1/WH): the approximate reciprocal (<= 1 ulp) runs at
+                // full rate, the fast-division intrinsic at a third of it.  min(., FLT_MAX)
+                // keeps the zero-filled edges (V = 0, WH = 0) at 0 instead of 0 * inf.
                 float const vv = __uint_as_float(v[c]);
-                float const r = (vv == 0.0f) ? 0.0f : __fdividef(vv, __uint_as_float(d[c]));
+                float const r = vv * fminf(rcp_approx(__uint_as_float(d[c])), FLT_MAX);
                 float const h = tf32_rna(r);
 #ifdef NMFB_FUSED_DEBUG
                 if (args.dbg && blockIdx.x == 0 && t == 0) {
@@ -609,6 +682,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 d[c] = __float_as_uint(h);
                 v[c] = __float_as_uint(r - h);
             }
+            DBG_PH(5, t);
             if (QW == 32) {
                 tmem_st32(lane_addr + dcol, d);
                 if (NTERMS == 3) tmem_st32(lane_addr + dcol + BR, v);
@@ -617,22 +691,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 if (NTERMS == 3) tmem_st16(lane_addr + dcol + BR, v);
             }
             tmem_wait_st();
+            DBG_PH(6, t);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&rfull[b]);
+            DBG_PH(7, t);
             if (warp == 4 && lane == 0) DBG_TS(6, t);
 #ifdef NMFB_FUSED_DEBUG
-            if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[512 + (warp - 4) * 64 + t] = globaltimer() - ts0;
+            if (lane == 0 && dts && blockIdx.x == 0 && t < 64 && warp < 12) dts[512 + (warp - 4) * 64 + t] = globaltimer() - ts0;
 #endif
         }
-    } else if (warp >= 12) {
+    } else if (warp >= 4 + NR) {
         // ------------------------------------------------------------ accumulator warps
-        // Warp 12+q owns TMEM lanes 32q..32q+31: sums the per-tile Acc into FP32
+        // Warp 4+NR+q owns TMEM lanes 32q..32q+31: sums the per-tile Acc into FP32
         // registers, and (all four together) splits X and the Y tiles.
         uint32_t const quad = warp & 3;
         uint32_t const row = quad * 32 + lane;
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
-        uint32_t const atid = (warp - 12) * 32 + lane;  // 0..127, for the cooperative splits
+        uint32_t const atid = (warp - 4 - NR) * 32 + lane;  // 0..127, for the cooperative splits
         float sum[KP];
 #pragma unroll
         for (int c = 0; c < KP; c++) sum[c] = 0.0f;
@@ -642,7 +718,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             if (!mbar_wait(&yraw[s], (ty / G::YST) & 1, abort_flag, args.err, 11u)) return false;
             unsigned char *syh = sY + s * G::YSTAGE;
             unsigned char *syth = sYT + s * G::YTSTAGE;
-            split_tile<KP>(syh, syh + G::YBYTES, syth, syth + G::YBYTES, BR, G::YBLK, atid, 128);
+            split_tile<KP>(syh, syh + G::YBYTES, syth, BR, G::YBLK, atid, 128);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&yready[s]);
@@ -650,7 +726,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         };
         bool ok = mbar_wait(xraw, 0, abort_flag, args.err, 10u);
         if (ok) {
-            split_tile<KP>(sXh, sXl, nullptr, nullptr, BO, G::XBLK, atid, 128);
+            split_tile<KP>(sXh, sXl, nullptr, BO, G::XBLK, atid, 128);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(xready);
@@ -660,25 +736,26 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             uint32_t const bp = t & 1;
             if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
             tc_fence_after();
+            // Acc columns [0, KP) and, for the 3-term arm, [KP, 2 KP) both add to sum.
 #pragma unroll
-            for (int c0 = 0; c0 < KP; c0 += 32) {
-                uint32_t a[32];
-                if (KP - c0 >= 32)
-                    tmem_ld32(lane_addr + bp * ACC_COLS + c0, a);
-                else
-                    tmem_ld16(lane_addr + bp * ACC_COLS + c0, a);
-                tmem_wait_ld_dep(a);
+            for (int part = 0; part < (NTERMS == 3 ? 2 : 1); part++) {
 #pragma unroll
-                for (int c = 0; c < 32 && c0 + c < KP; c++) sum[c0 + c] += __uint_as_float(a[c]);
+                for (int c0 = 0; c0 < KP; c0 += 16) {
+                    uint32_t a[32];
+                    tmem_ld16(lane_addr + bp * ACC_COLS + part * KP + c0, a);
+                    tmem_wait_ld_dep(a);
+#pragma unroll
+                    for (int c = 0; c < 16; c++) sum[c0 + c] += __uint_as_float(a[c]);
+                }
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&accfree[bp]);
-            if (warp == 12 && lane == 0) DBG_TS(7, t);
+            if (warp == 4 + NR && lane == 0) DBG_TS(7, t);
             // MMA2(t) has completed, so its Y^T stage (t % YST) is free: prepare Y(t + YST).
             if (t + G::YST < T && !split_y(t + G::YST)) { ok = false; break; }
 #ifdef NMFB_FUSED_DEBUG
-            if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[1024 + (warp - 12) * 64 + t] = globaltimer() - ts0;
+            if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[1024 + (warp - 4 - NR) * 64 + t] = globaltimer() - ts0;
 #endif
         }
         if (ok) {
@@ -695,7 +772,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
         }
     }
-    if (T == 0 && warp >= 12) {
+    if (T == 0 && warp >= 4 + NR) {
         uint32_t const o = o0 + (warp & 3) * 32 + lane;
         if (o < args.O) {
             float *dst = args.part + ((size_t)split * args.O + o) * KP;
@@ -783,7 +860,7 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
     int const main = HSIDE ? 0 : 1;
     int rc = nmfb_prof_begin(ctx, main);
     if (rc) return rc;
-    kern<<<oblocks * nsplit, NTHREADS, G::SMEM, ctx->stream>>>(maps, args);
+    kern<<<oblocks * nsplit, G::NTHR, G::SMEM, ctx->stream>>>(maps, args);
     NMFB_LAUNCH_CHECK(ctx);
     if ((rc = nmfb_prof_end(ctx, main))) return rc;
     return (int)nsplit;
@@ -849,8 +926,8 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused error word: %s", cudaGetErrorString(e));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
 #ifdef NMFB_FUSED_DEBUG
-    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (4 * BO * 64 + 4096) * sizeof(float)));
-    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (4 * BO * 64 + 4096) * sizeof(float), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (4 * BO * 64 + 8192) * sizeof(float)));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (4 * BO * 64 + 8192) * sizeof(float), ctx->stream));
 #endif
     uint32_t const cb = (kp == 16) ? 16 : 32;
     CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
@@ -896,7 +973,7 @@ int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
 extern "C" int nmfb_debug_dump(nmfb_ctx *ctx, float *host)
 {
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
-    NMFB_CUDA_TRY(ctx, cudaMemcpy(host, plan->dDbg, (4 * BO * 64 + 4096) * sizeof(float), cudaMemcpyDeviceToHost));
+    NMFB_CUDA_TRY(ctx, cudaMemcpy(host, plan->dDbg, (4 * BO * 64 + 8192) * sizeof(float), cudaMemcpyDeviceToHost));
     return NMFB_OK;
 }
 #endif
