@@ -36,7 +36,7 @@ ARM_FUSED_TF32 = 2
 ARMS = {"fused": ARM_FUSED, "plain": ARM_PLAIN, "fused_tf32": ARM_FUSED_TF32}
 
 NMFB_OK = 0
-_ERRNAMES = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENODEV", -5: "ESTATE", -6: "ETIMEOUT"}
+_ERRNAMES = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENODEV", -5: "ESTATE", -6: "ETIMEOUT", -7: "ETOOBIG"}
 
 
 class NMFError(RuntimeError):
@@ -86,6 +86,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_profile_read": ([vp, i32, C.POINTER(C.c_double), C.POINTER(u32)], i32),
         "nmfb_synchronize": ([vp], i32),
         "nmfb_launch_count": ([vp], C.c_uint64),
+        "nmfb_update_H_noalloc": ([vp, sz, vp, sz, vp, sz, u32, u32, u32, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -97,6 +98,33 @@ def load_library(path: str = LIB_PATH):
 
 def device_count() -> int:
     return int(load_library().nmfb_device_count())
+
+
+NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
+NOALLOC_MAX_MK = 4186112
+
+
+def update_H_noalloc(V: int, ldv: int, W: int, ldw: int, H: int, ldh: int, n: int, m: int, k: int,
+                     stream: int | None = None) -> None:
+    """update_H on caller-owned device buffers, allocating nothing.
+
+    For callers that must not allocate device memory (a framework whose caching
+    allocator owns the HBM, a plugin host that hands out every buffer, a loop
+    that cannot take cudaFree's device-wide synchronisation).  ``V``, ``W`` and
+    ``H`` are device addresses (e.g. ``tensor.data_ptr()``) on the current
+    device: V is n x m, W is n x k, H is m x k and is updated in place.  The
+    work is queued on ``stream`` (a raw cudaStream_t handle; None = default
+    stream) and this returns before it finishes.  Limits: k <= 64 and
+    m * k <= NOALLOC_MAX_MK (NMFError ETOOBIG beyond).  Calls share one fixed
+    16 MiB device scratch array, so calls that overlap on the GPU race; the
+    first call on a device looks up that array and belongs before any stream
+    capture.
+    """
+    rc = load_library().nmfb_update_H_noalloc(V, ldv, W, ldw, H, ldh, n, m, k, stream or None)
+    if rc != NMFB_OK:
+        why = {-1: "invalid pointer, rank or leading dimension",
+               -7: f"m*k = {m * k} exceeds the fixed scratch (k <= 64, m*k <= {NOALLOC_MAX_MK})"}
+        raise NMFError(rc, why.get(rc, "CUDA error or no sm_100 device"))
 
 
 def _fptr(a: np.ndarray):

@@ -36,6 +36,7 @@ extern "C" {
 #define NMFB_ENODEV (-4)   /* no sm_100 device / extension not usable */
 #define NMFB_ESTATE (-5)   /* call out of order (e.g. update before V is set) */
 #define NMFB_ETIMEOUT (-6) /* a bounded device wait ran out */
+#define NMFB_ETOOBIG (-7)  /* problem larger than nmfb_update_H_noalloc's fixed scratch */
 
 /* Update kernels ("arms").  All arms run the same method; they differ only
  * in how the two n x m x k contractions of a half-iteration are evaluated. */
@@ -158,6 +159,38 @@ int nmfb_synchronize(nmfb_ctx *ctx);
 
 /* Kernel launches issued by this context since creation (for accounting). */
 uint64_t nmfb_launch_count(const nmfb_ctx *ctx);
+
+/* ---------------------------------------------------------------------------
+ * update_H without any allocation.  No counterpart in the reference: it is an
+ * addition of this library for callers that must not allocate device memory,
+ * such as a host framework whose caching allocator already owns the HBM, a
+ * plugin host that hands out every device buffer itself, or a latency-bound
+ * loop that cannot take the device-wide synchronisation of cudaFree.
+ *
+ * Computes H = H .* (W' (V ./ (W H))) ./ colsum(W), the same update as
+ * nmfb_update_H (results agree to FP32 rounding), on caller-owned DEVICE
+ * buffers of the calling thread's current device: V (n x m, ldv >= m),
+ * W (n x k, ldw >= k) and H (m x k, ldh >= k, updated in place).  The work is
+ * queued on `stream` (a cudaStream_t as void*, NULL = default stream) and the
+ * call returns without waiting for it.
+ *
+ * It calls no cudaMalloc, cudaFree or allocating library routine.  Its scratch
+ * is one file-scope device array of NMFB_NOALLOC_SCRATCH_BYTES (16 MiB) that
+ * every GPU which loads this library holds until the process exits.  Limits:
+ * 1 <= k <= 64 and m * k <= NMFB_NOALLOC_MAX_MK; larger problems are rejected
+ * with NMFB_ETOOBIG before any work is queued (invalid pointers, ranks or
+ * leading dimensions give NMFB_EINVAL).
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any stream
+ * capture.  All calls share the one array and no state carries over between
+ * them, but calls whose work overlaps on the GPU (other streams, other host
+ * threads) race on it: serialise them.
+ */
+#define NMFB_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+#define NMFB_NOALLOC_MAX_MK 4186112u /* (16 MiB - 32 KiB of column sums) / 4 bytes */
+int nmfb_update_H_noalloc(const float *V, size_t ldv, const float *W, size_t ldw, float *H, size_t ldh,
+                          uint32_t n, uint32_t m, uint32_t k, void *stream);
 
 #ifdef __cplusplus
 }
