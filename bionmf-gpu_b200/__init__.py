@@ -87,6 +87,18 @@ def load_library(path: str = LIB_PATH):
         "nmfb_synchronize": ([vp], i32),
         "nmfb_launch_count": ([vp], C.c_uint64),
         "nmfb_update_H_noalloc": ([vp, sz, vp, sz, vp, sz, u32, u32, u32, vp], i32),
+        "nmfb_batch_create": ([C.POINTER(vp), i32, u32, u32, u32, C.POINTER(u32)], i32),
+        "nmfb_batch_destroy": ([vp], i32),
+        "nmfb_batch_last_error": ([vp], C.c_char_p),
+        "nmfb_batch_set_V": ([vp, fp, sz], i32),
+        "nmfb_batch_init_random": ([vp, C.POINTER(u32)], i32),
+        "nmfb_batch_set_WH": ([vp, u32, fp, sz, fp, sz], i32),
+        "nmfb_batch_set_tiles": ([vp, u32, u32, u32], i32),
+        "nmfb_batch_run": ([vp, u32, u32, u32, C.POINTER(u32), C.POINTER(i32)], i32),
+        "nmfb_batch_last_ms": ([vp, C.POINTER(C.c_double)], i32),
+        "nmfb_batch_get_classification": ([vp, C.POINTER(u32)], i32),
+        "nmfb_batch_get_WH": ([vp, u32, fp, sz, fp, sz], i32),
+        "nmfb_batch_consensus": ([vp, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_double)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -270,6 +282,111 @@ class NMF:
 
     def launch_count(self) -> int:
         return int(self._L.nmfb_launch_count(self._h))
+
+
+def _uptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+class Batch:
+    """Many independent solves of one V (n x m): problem p has rank ranks[p].
+
+    All problems run the reference's loop in one persistent launch
+    (``run``); ``consensus(k)`` summarises the restarts of rank k.
+    """
+
+    def __init__(self, n: int, m: int, ranks, device: int = 0):
+        self._L = load_library()
+        self.n, self.m = int(n), int(m)
+        self.ranks = np.ascontiguousarray(ranks, np.uint32)
+        self.nprob = int(self.ranks.shape[0])
+        self._h = C.c_void_p()
+        rc = self._L.nmfb_batch_create(C.byref(self._h), device, self.n, self.m, self.nprob, _uptr(self.ranks))
+        if rc != NMFB_OK:
+            msg = self._L.nmfb_batch_last_error(self._h).decode() if self._h.value else "batch creation failed"
+            self._L.nmfb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+            raise NMFError(rc, msg)
+
+    def _check(self, rc: int):
+        if rc != NMFB_OK:
+            raise NMFError(rc, self._L.nmfb_batch_last_error(self._h).decode())
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            self._L.nmfb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_V(self, V: np.ndarray):
+        V = np.ascontiguousarray(V, np.float32)
+        assert V.shape == (self.n, self.m)
+        self._check(self._L.nmfb_batch_set_V(self._h, _fptr(V), self.m))
+
+    def init_random(self, seeds):
+        seeds = np.ascontiguousarray(seeds, np.uint32)
+        assert seeds.shape == (self.nprob,)
+        self._check(self._L.nmfb_batch_init_random(self._h, _uptr(seeds)))
+
+    def set_WH(self, p: int, W: np.ndarray, H: np.ndarray):
+        W = np.ascontiguousarray(W, np.float32)
+        H = np.ascontiguousarray(H, np.float32)
+        k = int(self.ranks[p])
+        assert W.shape == (self.n, k) and H.shape == (self.m, k)
+        self._check(self._L.nmfb_batch_set_WH(self._h, p, _fptr(W), k, _fptr(H), k))
+
+    def set_tiles(self, p: int, wt: int, jt: int):
+        self._check(self._L.nmfb_batch_set_tiles(self._h, p, wt, jt))
+
+    def run(self, n_iters=2000, niter_test_conv=10, stop_threshold=40):
+        """Returns (iterations, converged) arrays, one entry per problem."""
+        it = np.zeros(self.nprob, np.uint32)
+        cv = np.zeros(self.nprob, np.int32)
+        self._check(self._L.nmfb_batch_run(self._h, n_iters, niter_test_conv, stop_threshold, _uptr(it),
+                                           cv.ctypes.data_as(C.POINTER(C.c_int))))
+        return it, cv.astype(bool)
+
+    def last_ms(self) -> float:
+        ms = C.c_double()
+        self._check(self._L.nmfb_batch_last_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def classification(self) -> np.ndarray:
+        out = np.empty((self.nprob, self.m), np.uint32)
+        self._check(self._L.nmfb_batch_get_classification(self._h, _uptr(out)))
+        return out
+
+    def W(self, p: int) -> np.ndarray:
+        k = int(self.ranks[p])
+        out = np.empty((self.n, k), np.float32)
+        self._check(self._L.nmfb_batch_get_WH(self._h, p, _fptr(out), k, None, k))
+        return out
+
+    def H(self, p: int) -> np.ndarray:
+        k = int(self.ranks[p])
+        out = np.empty((self.m, k), np.float32)
+        self._check(self._L.nmfb_batch_get_WH(self._h, p, None, k, _fptr(out), k))
+        return out
+
+    def consensus(self, k: int, cophenetic: bool = True):
+        """(counts m x m uint32, nruns, cophenetic correlation or None) of the rank-k problems."""
+        counts = np.empty((self.m, self.m), np.uint32)
+        nruns = C.c_uint32()
+        coph = C.c_double()
+        self._check(self._L.nmfb_batch_consensus(self._h, k, _uptr(counts), C.byref(nruns),
+                                                 C.byref(coph) if cophenetic else None))
+        return counts, int(nruns.value), (coph.value if cophenetic else None)
 
 
 def nmf_gpu(V: np.ndarray, k: int = 2, n_iters: int = 2000, niter_test_conv: int = 10, stop_threshold: int = 40,

@@ -1,0 +1,995 @@
+// batch.cu -- many independent KL-NMF solves in one persistent launch
+// (rank-selection and restart sweeps), with exact integer consensus matrices
+// and the FP64 cophenetic correlation of each rank's restarts.
+//
+// Every problem runs the reference's complete loop (src/NMF_GPU.c:522-795):
+// update_H, update_W; after every niter_test_conv iterations the EPS adjust of
+// W (fused into the block's last update_W) and of H (fused into the
+// classification), the argmax classification with the reference's lane-exact
+// tie rule (src/GPU_kernels.cu:2508-2656, 3177-3267) and the connectivity test
+// (src/common.c:1195-1209) with the stop rule of src/NMF_GPU.c:695-709; the
+// remaining n_iters % niter_test_conv iterations run without adjust.
+//
+// Work distribution: persistent CTAs (occupancy x SMs, at most one per
+// problem) take problems from an atomic work queue in the order the host gives
+// (largest rank first), and one CTA runs one problem to its end.  Problems are
+// independent, so no CTA ever waits on another.
+//
+// Per problem, in one CTA of NT = 256 threads:
+//   shared memory: H (m x ks, ks = k rounded up to 4), a staging tile (rows of
+//                  W for update_H, or an NT x (jt+1) tile of V for update_W),
+//                  colsum vectors, labels and the previous partition;
+//   global memory: V (n x ldv, shared by all problems of a sweep, L2-resident
+//                  at sweep sizes) and W (n x ks, padding columns zero).
+//   update_H: thread j owns sample j: h_j in registers, WH_ij = W_i . h_j with
+//             W_i broadcast from the staged tile, Haux_j += (V_ij / WH_ij) W_i,
+//             summed per tile of wt rows and then across tiles;
+//             H_j = (H_j .* Haux_j) ./ colsum(W)   (product first, then a
+//             correctly-rounded division, as kernel_mul_div);
+//   update_W: thread i owns row i: W_i in registers, V staged through shared
+//             memory in NT x jt tiles (coalesced loads, conflict-free reads),
+//             H_j broadcast from shared memory; same formulas mirrored.
+//   colsum(W) and colsum(H) are reduced from the rows each thread just wrote,
+//   in a fixed order (warp shuffles, then warps in order).
+// Ranks 2..20 are compiled as exact-rank instantiations (no padded flops).
+// Tile shapes (wt, jt) are per-problem values (nmfb_batch_set_tiles; the
+// Python layer's autotuner picks them per (k, m) bucket).
+#include "nmfb_internal.cuh"
+
+#include <float.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <algorithm>
+#include <new>
+#include <vector>
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int NW = NT / 32;
+constexpr uint32_t KMIN = 2, KMAX = 20;
+
+struct Problem {
+    const float *V;      // n x ldv
+    float *W;            // n x ks
+    float *H;            // m x ks
+    uint32_t *labels;    // m: classification of the final H
+    uint64_t ldv;
+    uint32_t n, m, k, ks;
+    uint32_t wt, jt;     // tile shapes
+    uint32_t iterations; // out
+    uint32_t converged;  // out
+    uint32_t tests;      // out: convergence tests performed
+    uint32_t pad;
+};
+
+struct LoopArgs {
+    uint32_t n_iters, niter_test_conv, stop_threshold;
+};
+
+__host__ __device__ constexpr uint32_t ks_of(uint32_t k) { return (k + 3u) & ~3u; }
+
+// Shared-memory layout of one problem (offsets in floats).  The staging region
+// holds two buffers (double buffering) of either phase:
+//   update_H: V rows [i0, i0+wt) x columns [j0, j0+cs) (cs = min(NT, ldv)) and
+//             W rows [i0, i0+wt) (wt x ks);
+//   update_W: V rows [i0, i0+NT) x columns [j0, j0+jt), row stride jt + 4
+//             (16-byte aligned rows; float4 reads of 8 consecutive rows hit
+//             8 distinct bank groups).
+struct SmemLayout {
+    uint32_t h, stage, red, accw, acch, lab, rep, first, total;
+    uint32_t cs, hbuf, wbuf, vst;   // update_H column span and buffer sizes; update_W row stride
+};
+__host__ __device__ inline SmemLayout smem_layout(uint32_t m, uint32_t ks, uint32_t wt, uint32_t jt, uint64_t ldv)
+{
+    SmemLayout L;
+    L.cs = ldv < (uint64_t)NT ? (uint32_t)ldv : (uint32_t)NT;
+    L.hbuf = wt * (L.cs + ks);
+    L.vst = jt + 4;
+    L.wbuf = NT * L.vst;
+    uint32_t const stage = 2u * (L.hbuf > L.wbuf ? L.hbuf : L.wbuf);
+    L.h = 0;
+    L.stage = (m * ks + 3u) & ~3u;
+    L.red = L.stage + stage;
+    L.accw = L.red + NW * ks;
+    L.acch = L.accw + ks;
+    L.lab = L.acch + ks;
+    L.rep = L.lab + m;
+    L.first = L.rep + m;
+    L.total = L.first + 32;
+    return L;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    uint32_t const s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// 1/x with rcp.approx.ftz.f32 (PTX: at most 1 ulp of error); the quotient is
+// v * min(1/wh, FLT_MAX), so a zero denominator gives a finite result.
+__device__ __forceinline__ float quotient(float v, float wh)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(wh));
+    return v * fminf(r, FLT_MAX);
+}
+
+// Load the first K of a 16-byte aligned row of KS floats with float4 loads.
+template <int K>
+__device__ __forceinline__ void load_row(const float *p, float (&x)[K])
+{
+    constexpr int KS = (int)ks_of(K);
+#pragma unroll
+    for (int q = 0; q < KS / 4; q++) {
+        float4 const f = reinterpret_cast<const float4 *>(p)[q];
+        if (4 * q + 0 < K) x[4 * q + 0] = f.x;
+        if (4 * q + 1 < K) x[4 * q + 1] = f.y;
+        if (4 * q + 2 < K) x[4 * q + 2] = f.z;
+        if (4 * q + 3 < K) x[4 * q + 3] = f.w;
+    }
+}
+
+// One element of a contraction: wh = a . b, q = v / wh, acc += q * b.
+template <int K>
+__device__ __forceinline__ void element(float v, const float (&a)[K], const float (&b)[K], float (&acc)[K])
+{
+    float wh = 0.0f;
+#pragma unroll
+    for (int c = 0; c < K; c++) wh = fmaf(a[c], b[c], wh);
+    float const q = quotient(v, wh);
+#pragma unroll
+    for (int c = 0; c < K; c++) acc[c] = fmaf(q, b[c], acc[c]);
+}
+
+// Sum v[0..K) over the CTA in a fixed order; thread c < K writes out[c].
+template <int K>
+__device__ __forceinline__ void block_sum(float (&v)[K], float *red, float *out, uint32_t ks)
+{
+    uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < K; c++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], off);
+    if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < K; c++) red[warp * ks + c] = v[c];
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)K) {
+        float s = 0.0f;
+        for (int w = 0; w < NW; w++) s += red[w * ks + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// update_H: stage tile t (rows of V for columns [j0, j0+cs) and rows of W) into buffer b.
+template <uint32_t KS>
+__device__ __forceinline__ void stage_H(const Problem &P, float *buf, const SmemLayout &L, uint32_t j0, uint32_t i0,
+                                        uint32_t rows)
+{
+    uint32_t const q4 = L.cs / 4;
+    float *sV = buf, *sW = buf + P.wt * L.cs;
+    for (uint32_t e = threadIdx.x; e < rows * q4; e += NT) {
+        uint32_t const r = e / q4, q = e - r * q4;
+        if (j0 + 4 * q < P.ldv) cp_async16(sV + r * L.cs + 4 * q, P.V + (size_t)(i0 + r) * P.ldv + j0 + 4 * q);
+    }
+    const float *src = P.W + (size_t)i0 * KS;
+    for (uint32_t e = threadIdx.x; e < rows * (KS / 4); e += NT) cp_async16(sW + 4 * e, src + 4 * e);
+}
+
+template <int K>
+__device__ void update_H(const Problem &P, float *sm, const SmemLayout &L)
+{
+    constexpr uint32_t KS = ks_of(K);
+    float *sH = sm + L.h;
+    float *stage = sm + L.stage;
+    uint32_t const half = (L.hbuf > L.wbuf ? L.hbuf : L.wbuf);
+    const float *accW = sm + L.accw;
+    uint32_t const tid = threadIdx.x, n = P.n, m = P.m, wt = P.wt;
+    uint32_t const ntiles = (n + wt - 1) / wt;
+    float hsum[K];
+#pragma unroll
+    for (int c = 0; c < K; c++) hsum[c] = 0.0f;
+    for (uint32_t j0 = 0; j0 < m; j0 += NT) {
+        uint32_t const j = j0 + tid;
+        bool const active = j < m;
+        float h[K], acc[K];
+#pragma unroll
+        for (int c = 0; c < K; c++) {
+            h[c] = active ? sH[j * KS + c] : 0.0f;
+            acc[c] = 0.0f;
+        }
+        __syncthreads();   // the staging region may still be read by the previous phase
+        stage_H<KS>(P, stage, L, j0, 0, min(wt, n));
+        cp_async_commit();
+        for (uint32_t t = 0; t < ntiles; t++) {
+            uint32_t const i0 = t * wt;
+            uint32_t const rows = min(wt, n - i0);
+            if (t + 1 < ntiles) stage_H<KS>(P, stage + ((t + 1) & 1) * half, L, j0, i0 + wt, min(wt, n - i0 - wt));
+            cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();
+            const float *sV = stage + (t & 1) * half;
+            const float *sW = sV + wt * L.cs;
+            if (active) {
+                float tl[K];
+#pragma unroll
+                for (int c = 0; c < K; c++) tl[c] = 0.0f;
+#pragma unroll 4
+                for (uint32_t r = 0; r < rows; r++) {
+                    float w[K];
+                    load_row<K>(sW + r * KS, w);
+                    element<K>(sV[r * L.cs + tid], h, w, tl);
+                }
+#pragma unroll
+                for (int c = 0; c < K; c++) acc[c] += tl[c];
+            }
+            __syncthreads();
+        }
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < K; c++) {
+                float const hn = __fdiv_rn(h[c] * acc[c], accW[c]);
+                sH[j * KS + c] = hn;
+                hsum[c] += hn;
+            }
+        }
+    }
+    block_sum<K>(hsum, sm + L.red, sm + L.acch, KS);
+}
+
+// update_W: stage V rows [i0, i0+rows) x columns [j0, j0+jt) into buffer b (row stride vst).
+__device__ __forceinline__ void stage_W(const Problem &P, float *buf, const SmemLayout &L, uint32_t i0, uint32_t rows,
+                                        uint32_t j0)
+{
+    uint32_t const q4 = P.jt / 4;
+    for (uint32_t e = threadIdx.x; e < rows * q4; e += NT) {
+        uint32_t const r = e / q4, q = e - r * q4;
+        if (j0 + 4 * q < P.ldv) cp_async16(buf + r * L.vst + 4 * q, P.V + (size_t)(i0 + r) * P.ldv + j0 + 4 * q);
+    }
+}
+
+template <int K>
+__device__ void update_W(const Problem &P, float *sm, const SmemLayout &L, bool adjust)
+{
+    constexpr uint32_t KS = ks_of(K);
+    const float *sH = sm + L.h;
+    float *stage = sm + L.stage;
+    uint32_t const half = (L.hbuf > L.wbuf ? L.hbuf : L.wbuf);
+    const float *accH = sm + L.acch;
+    uint32_t const tid = threadIdx.x, n = P.n, m = P.m, jt = P.jt;
+    uint32_t const ntiles = (m + jt - 1) / jt;
+    float wsum[K];
+#pragma unroll
+    for (int c = 0; c < K; c++) wsum[c] = 0.0f;
+    for (uint32_t i0 = 0; i0 < n; i0 += NT) {
+        uint32_t const i = i0 + tid;
+        bool const active = i < n;
+        uint32_t const rows = min((uint32_t)NT, n - i0);
+        float w[K], aux[K];
+#pragma unroll
+        for (int c = 0; c < K; c++) {
+            w[c] = active ? P.W[(size_t)i * KS + c] : 0.0f;
+            aux[c] = 0.0f;
+        }
+        __syncthreads();   // the staging region may still be read by the previous phase
+        stage_W(P, stage, L, i0, rows, 0);
+        cp_async_commit();
+        for (uint32_t t = 0; t < ntiles; t++) {
+            uint32_t const j0 = t * jt;
+            uint32_t const cols = min(jt, m - j0);
+            if (t + 1 < ntiles) stage_W(P, stage + ((t + 1) & 1) * half, L, i0, rows, j0 + jt);
+            cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();
+            if (active) {
+                const float *vrow = stage + (t & 1) * half + tid * L.vst;
+                float tl[K];
+#pragma unroll
+                for (int c = 0; c < K; c++) tl[c] = 0.0f;
+                uint32_t const cols4 = cols & ~3u;
+                const float *hrow = sH + j0 * KS;
+                for (uint32_t jj = 0; jj < cols4; jj += 4) {
+                    float4 const v4 = *reinterpret_cast<const float4 *>(vrow + jj);
+                    float hj[K];
+                    load_row<K>(hrow + (jj + 0) * KS, hj);
+                    element<K>(v4.x, w, hj, tl);
+                    load_row<K>(hrow + (jj + 1) * KS, hj);
+                    element<K>(v4.y, w, hj, tl);
+                    load_row<K>(hrow + (jj + 2) * KS, hj);
+                    element<K>(v4.z, w, hj, tl);
+                    load_row<K>(hrow + (jj + 3) * KS, hj);
+                    element<K>(v4.w, w, hj, tl);
+                }
+                for (uint32_t jj = cols4; jj < cols; jj++) {
+                    float hj[K];
+                    load_row<K>(hrow + jj * KS, hj);
+                    element<K>(vrow[jj], w, hj, tl);
+                }
+#pragma unroll
+                for (int c = 0; c < K; c++) aux[c] += tl[c];
+            }
+            __syncthreads();
+        }
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < K; c++) {
+                float wn = __fdiv_rn(w[c] * aux[c], accH[c]);
+                if (adjust) wn = fmaxf(wn, FLT_MIN);
+                P.W[(size_t)i * KS + c] = wn;
+                wsum[c] += wn;
+            }
+        }
+    }
+    block_sum<K>(wsum, sm + L.red, sm + L.accw, KS);
+}
+
+// Warp-per-sample classification of H with the reference's tie rule (k <= 32:
+// lane t holds column t, idle lanes hold (-1, 0); xor butterfly 16..1, a lane
+// takes the other value only if it is strictly larger).  With `adjust`, H is
+// first clamped to FLT_MIN (the test's matrix_adjust).  Records first[label].
+template <int K>
+__device__ void classify(float *sm, const SmemLayout &L, uint32_t m, bool adjust)
+{
+    constexpr uint32_t KS = ks_of(K);
+    float *sH = sm + L.h;
+    uint32_t *lab = reinterpret_cast<uint32_t *>(sm + L.lab);
+    uint32_t *first = reinterpret_cast<uint32_t *>(sm + L.first);
+    uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t j = warp; j < m; j += NW) {
+        float v = -1.0f;
+        uint32_t id = 0;
+        if (lane < (uint32_t)K) {
+            float x = sH[j * KS + lane];
+            if (adjust) {
+                x = fmaxf(x, FLT_MIN);
+                sH[j * KS + lane] = x;
+            }
+            v = x;
+            id = lane;
+        }
+#pragma unroll
+        for (uint32_t half = 16; half > 0; half >>= 1) {
+            float const ov = __shfl_xor_sync(0xffffffffu, v, half);
+            uint32_t const oi = __shfl_xor_sync(0xffffffffu, id, half);
+            if (v < ov) {
+                v = ov;
+                id = oi;
+            }
+        }
+        if (lane == 0) {
+            lab[j] = id;
+            atomicMin(&first[id], j);
+        }
+    }
+    __syncthreads();
+}
+
+template <int K>
+__device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *s_ctl)
+{
+    constexpr uint32_t KS = ks_of(K);
+    SmemLayout const L = smem_layout(P.m, KS, P.wt, P.jt, P.ldv);
+    uint32_t const tid = threadIdx.x, m = P.m, n = P.n;
+    uint32_t *lab = reinterpret_cast<uint32_t *>(sm + L.lab);
+    uint32_t *rep = reinterpret_cast<uint32_t *>(sm + L.rep);
+    uint32_t *first = reinterpret_cast<uint32_t *>(sm + L.first);
+    // s_ctl[0] = inc, [1] = converged, [2] = tests
+
+    {
+        const float4 *src = reinterpret_cast<const float4 *>(P.H);
+        float4 *dst = reinterpret_cast<float4 *>(sm + L.h);
+        for (uint32_t e = tid; e < m * KS / 4; e += NT) dst[e] = src[e];
+    }
+    for (uint32_t j = tid; j < m; j += NT) rep[j] = 0u;   // the first test compares with an all-zero vector
+    if (tid < 32) first[tid] = 0xffffffffu;
+    if (tid == 0) {
+        s_ctl[0] = 0;
+        s_ctl[1] = 0;
+        s_ctl[2] = 0;
+    }
+    {   // colsum(W) of the initial W
+        float ws[K];
+#pragma unroll
+        for (int c = 0; c < K; c++) ws[c] = 0.0f;
+        for (uint32_t i = tid; i < n; i += NT)
+#pragma unroll
+            for (int c = 0; c < K; c++) ws[c] += P.W[(size_t)i * KS + c];
+        __syncthreads();
+        block_sum<K>(ws, sm + L.red, sm + L.accw, KS);
+    }
+
+    uint32_t const J = A.niter_test_conv;
+    uint32_t const nblocks = A.n_iters / J, rem = A.n_iters % J;
+    for (uint32_t b = 0; b < nblocks; b++) {
+        for (uint32_t it = 0; it < J; it++) {
+            update_H<K>(P, sm, L);
+            update_W<K>(P, sm, L, it + 1 == J);
+        }
+        classify<K>(sm, L, m, true);
+        uint32_t local = 0;
+        for (uint32_t j = tid; j < m; j += NT) {
+            uint32_t const r = first[lab[j]];
+            local |= (r != rep[j]) ? 1u : 0u;
+            rep[j] = r;
+        }
+        int const any = __syncthreads_or((int)local);
+        if (tid < 32) first[tid] = 0xffffffffu;
+        if (tid == 0) {
+            s_ctl[2] += 1;
+            if (any)
+                s_ctl[0] = 0;
+            else if (s_ctl[0] < A.stop_threshold)
+                s_ctl[0] += 1;
+            else
+                s_ctl[1] = 1;
+        }
+        __syncthreads();
+        if (s_ctl[1]) break;
+    }
+    if (!s_ctl[1])
+        for (uint32_t it = 0; it < rem; it++) {
+            update_H<K>(P, sm, L);
+            update_W<K>(P, sm, L, false);
+        }
+    // final classification (no adjust) and write-back
+    classify<K>(sm, L, m, false);
+    for (uint32_t j = tid; j < m; j += NT) P.labels[j] = lab[j];
+    {
+        const float4 *src = reinterpret_cast<const float4 *>(sm + L.h);
+        float4 *dst = reinterpret_cast<float4 *>(P.H);
+        for (uint32_t e = tid; e < m * KS / 4; e += NT) dst[e] = src[e];
+    }
+    if (tid == 0) {
+        P.converged = s_ctl[1];
+        P.tests = s_ctl[2];
+        P.iterations = s_ctl[1] ? s_ctl[2] * J : A.n_iters;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, const uint32_t *__restrict__ order,
+                                                 uint32_t nprob, uint32_t *__restrict__ queue, LoopArgs A)
+{
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    __shared__ uint32_t s_next;
+    __shared__ uint32_t s_ctl[4];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
+        __syncthreads();
+        uint32_t const q = s_next;
+        if (q >= nprob) break;
+        Problem P = probs[order[q]];
+        switch (P.k) {
+#define NMFB_BATCH_CASE(KK) \
+    case KK: run_problem<KK>(P, sm, A, s_ctl); break;
+            NMFB_BATCH_CASE(2) NMFB_BATCH_CASE(3) NMFB_BATCH_CASE(4) NMFB_BATCH_CASE(5) NMFB_BATCH_CASE(6)
+            NMFB_BATCH_CASE(7) NMFB_BATCH_CASE(8) NMFB_BATCH_CASE(9) NMFB_BATCH_CASE(10) NMFB_BATCH_CASE(11)
+            NMFB_BATCH_CASE(12) NMFB_BATCH_CASE(13) NMFB_BATCH_CASE(14) NMFB_BATCH_CASE(15) NMFB_BATCH_CASE(16)
+            NMFB_BATCH_CASE(17) NMFB_BATCH_CASE(18) NMFB_BATCH_CASE(19) NMFB_BATCH_CASE(20)
+#undef NMFB_BATCH_CASE
+            default: break;
+        }
+        if (threadIdx.x == 0) {
+            Problem *dst = probs + order[q];
+            dst->iterations = P.iterations;
+            dst->converged = P.converged;
+            dst->tests = P.tests;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Consensus: C[a][b] = number of runs r in `sel` with labels_r[a] == labels_r[b]
+// (exact integer co-clustering counts).  One CTA per row a.
+__global__ void k_consensus(const uint32_t *const *__restrict__ labels, const uint32_t *__restrict__ sel, uint32_t nsel,
+                            uint32_t m, uint32_t *__restrict__ C)
+{
+    uint32_t const a = blockIdx.x;
+    for (uint32_t b = threadIdx.x; b < m; b += blockDim.x) {
+        uint32_t cnt = 0;
+        for (uint32_t s = 0; s < nsel; s++) {
+            const uint32_t *l = labels[sel[s]];
+            cnt += (l[a] == l[b]) ? 1u : 0u;
+        }
+        C[(size_t)a * m + b] = cnt;
+    }
+}
+
+__device__ __forceinline__ double consensus_distance(uint32_t c, double runs)
+{
+    return __dsub_rn(1.0, __ddiv_rn((double)c, runs));
+}
+
+// Cophenetic correlation (Brunet et al., PNAS 2004) of the consensus C over
+// nruns runs, in FP64, one CTA of 1024 threads:
+//   D = 1 - C / nruns (zero diagonal);
+//   average-linkage (UPGMA) agglomeration: repeatedly merge the two active
+//   clusters at the smallest distance, the lowest (a, b) slot pair first on
+//   ties; the merged cluster keeps slot a and its distance to x becomes
+//   (|a| D[a][x] + |b| D[b][x]) / (|a| + |b|); the cophenetic distance of two
+//   samples is the height at which their clusters merge;
+//   result = Pearson correlation of D and the cophenetic distances over all
+//   pairs a < b (means first, then centred sums).
+// Work buffers (global): Dw (m*m), coph (m*m); cid, csize (m each).
+__global__ void __launch_bounds__(1024) k_cophenetic(const uint32_t *__restrict__ C, uint32_t m, uint32_t nruns,
+                                                     double *__restrict__ Dw, double *__restrict__ coph,
+                                                     uint32_t *__restrict__ cid, uint32_t *__restrict__ csize,
+                                                     double *__restrict__ out)
+{
+    __shared__ double s_d[1024];
+    __shared__ uint32_t s_a[1024], s_b[1024];
+    __shared__ double s_r[3][1024];
+    uint32_t const tid = threadIdx.x, nt = blockDim.x;
+    double const runs = (double)nruns;
+    size_t const mm = (size_t)m * m;
+    for (size_t e = tid; e < mm; e += nt) {
+        uint32_t const a = (uint32_t)(e / m), b = (uint32_t)(e % m);
+        Dw[e] = (a == b) ? 0.0 : consensus_distance(C[e], runs);
+        coph[e] = 0.0;
+    }
+    for (uint32_t a = tid; a < m; a += nt) {
+        cid[a] = a;
+        csize[a] = 1;
+    }
+    __syncthreads();
+    for (uint32_t step = 0; step + 1 < m; step++) {
+        double best = INFINITY;
+        uint32_t ba = 0xffffffffu, bb = 0xffffffffu;
+        for (size_t e = tid; e < mm; e += nt) {
+            uint32_t const a = (uint32_t)(e / m), b = (uint32_t)(e % m);
+            if (a < b && csize[a] && csize[b]) {
+                double const d = Dw[e];
+                if (d < best) {   // e grows with (a, b): the first strict minimum is the lowest pair
+                    best = d;
+                    ba = a;
+                    bb = b;
+                }
+            }
+        }
+        s_d[tid] = best;
+        s_a[tid] = ba;
+        s_b[tid] = bb;
+        __syncthreads();
+        for (uint32_t s = nt / 2; s > 0; s >>= 1) {
+            if (tid < s) {
+                double const od = s_d[tid + s];
+                uint32_t const oa = s_a[tid + s], ob = s_b[tid + s];
+                if (od < s_d[tid] || (od == s_d[tid] && (oa < s_a[tid] || (oa == s_a[tid] && ob < s_b[tid])))) {
+                    s_d[tid] = od;
+                    s_a[tid] = oa;
+                    s_b[tid] = ob;
+                }
+            }
+            __syncthreads();
+        }
+        uint32_t const A = s_a[0], B = s_b[0];
+        double const h = s_d[0];
+        double const na = (double)csize[A], nb = (double)csize[B];
+        __syncthreads();
+        for (size_t e = tid; e < mm; e += nt) {
+            uint32_t const a = (uint32_t)(e / m), b = (uint32_t)(e % m);
+            uint32_t const ca = cid[a], cb = cid[b];
+            if ((ca == A && cb == B) || (ca == B && cb == A)) coph[e] = h;
+        }
+        __syncthreads();
+        for (uint32_t x = tid; x < m; x += nt) {
+            if (x != A && x != B && csize[x]) {
+                double const d = __ddiv_rn(__dadd_rn(__dmul_rn(na, Dw[(size_t)A * m + x]), __dmul_rn(nb, Dw[(size_t)B * m + x])),
+                                           __dadd_rn(na, nb));
+                Dw[(size_t)A * m + x] = d;
+                Dw[(size_t)x * m + A] = d;
+            }
+        }
+        __syncthreads();
+        for (uint32_t x = tid; x < m; x += nt)
+            if (cid[x] == B) cid[x] = A;
+        if (tid == 0) {
+            csize[A] += csize[B];
+            csize[B] = 0;
+        }
+        __syncthreads();
+    }
+    // Pearson correlation over a < b: means, then centred sums.
+    double const np = (double)m * (double)(m - 1) / 2.0;
+    double sx = 0.0, sy = 0.0;
+    for (size_t e = tid; e < mm; e += nt) {
+        uint32_t const a = (uint32_t)(e / m), b = (uint32_t)(e % m);
+        if (a < b) {
+            sx += consensus_distance(C[e], runs);
+            sy += coph[e];
+        }
+    }
+    s_r[0][tid] = sx;
+    s_r[1][tid] = sy;
+    __syncthreads();
+    for (uint32_t s = nt / 2; s > 0; s >>= 1) {
+        if (tid < s) {
+            s_r[0][tid] += s_r[0][tid + s];
+            s_r[1][tid] += s_r[1][tid + s];
+        }
+        __syncthreads();
+    }
+    double const mx = s_r[0][0] / np, my = s_r[1][0] / np;
+    __syncthreads();
+    double cxy = 0.0, cxx = 0.0, cyy = 0.0;
+    for (size_t e = tid; e < mm; e += nt) {
+        uint32_t const a = (uint32_t)(e / m), b = (uint32_t)(e % m);
+        if (a < b) {
+            double const x = consensus_distance(C[e], runs) - mx;
+            double const y = coph[e] - my;
+            cxy += x * y;
+            cxx += x * x;
+            cyy += y * y;
+        }
+    }
+    s_r[0][tid] = cxy;
+    s_r[1][tid] = cxx;
+    s_r[2][tid] = cyy;
+    __syncthreads();
+    for (uint32_t s = nt / 2; s > 0; s >>= 1) {
+        if (tid < s)
+            for (int q = 0; q < 3; q++) s_r[q][tid] += s_r[q][tid + s];
+        __syncthreads();
+    }
+    if (tid == 0) out[0] = (s_r[1][0] > 0.0 && s_r[2][0] > 0.0) ? s_r[0][0] / sqrt(s_r[1][0] * s_r[2][0]) : 0.0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct nmfb_batch {
+    int device;
+    cudaStream_t stream;
+    uint32_t n, m, nprob;
+    size_t ldv;
+    int sm_count;
+    size_t smem_optin;
+    std::vector<uint32_t> ranks;
+    std::vector<uint32_t> wt, jt;        // per-problem tile shapes
+    float *dV;
+    float *dW, *dH;                       // per-problem slices (n x ks, m x ks)
+    std::vector<size_t> woff, hoff;       // float offsets of each problem's slices
+    uint32_t *dLabels;                    // nprob x m
+    Problem *dProbs;
+    uint32_t *dOrder, *dQueue;
+    uint32_t **dLabelPtrs;
+    int v_set, wh_set;
+    cudaEvent_t ev0, ev1;
+    float last_ms;
+    char err[512];
+};
+
+static int bfail(nmfb_batch *b, int code, const char *fmt, ...)
+{
+    if (b) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(b->err, sizeof(b->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define BTRY(b, call)                                                                                      \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return bfail((b), NMFB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+static size_t problem_smem_bytes(uint32_t m, uint32_t k, uint32_t wt, uint32_t jt)
+{
+    uint64_t const ldv = ((uint64_t)m + 31) / 32 * 32;
+    return (size_t)smem_layout(m, ks_of(k), wt, jt, ldv).total * sizeof(float);
+}
+
+// Default tile shapes: wt rows of W per update_H tile, jt columns of V per update_W tile.
+static void default_tiles(uint32_t k, uint32_t m, uint32_t *wt, uint32_t *jt)
+{
+    (void)k;
+    *wt = 32;
+    *jt = m >= 64 ? 32 : 16;
+}
+
+static Problem make_problem(const nmfb_batch *b, uint32_t p)
+{
+    Problem P;
+    memset(&P, 0, sizeof(P));
+    uint32_t const k = b->ranks[p];
+    P.V = b->dV;
+    P.W = b->dW + b->woff[p];
+    P.H = b->dH + b->hoff[p];
+    P.labels = b->dLabels + (size_t)p * b->m;
+    P.ldv = b->ldv;
+    P.n = b->n;
+    P.m = b->m;
+    P.k = k;
+    P.ks = ks_of(k);
+    P.wt = b->wt[p];
+    P.jt = b->jt[p];
+    return P;
+}
+
+extern "C" {
+
+int nmfb_batch_create(nmfb_batch **out, int device, uint32_t n, uint32_t m, uint32_t nprob, const uint32_t *ranks)
+{
+    if (!out) return NMFB_EINVAL;
+    *out = nullptr;
+    nmfb_batch *b = new (std::nothrow) nmfb_batch();
+    if (!b) return NMFB_ENOMEM;
+    *out = b;
+    b->device = device;
+    if (n < 2 || m < 2 || nprob == 0 || !ranks) return bfail(b, NMFB_EINVAL, "invalid batch dimensions");
+    for (uint32_t p = 0; p < nprob; p++)
+        if (ranks[p] < KMIN || ranks[p] > KMAX || ranks[p] > (n < m ? n : m))
+            return bfail(b, NMFB_EINVAL, "problem %u: factorization rank %u must be in [2, min(%u, n, m)]", p, ranks[p],
+                         KMAX);
+    b->n = n;
+    b->m = m;
+    b->nprob = nprob;
+    b->ldv = ((size_t)m + 31) / 32 * 32;
+    b->ranks.assign(ranks, ranks + nprob);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return bfail(b, NMFB_ENODEV, "no CUDA device %d", device);
+    }
+    cudaDeviceProp prop;
+    BTRY(b, cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return bfail(b, NMFB_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a", device, prop.major, prop.minor);
+    BTRY(b, cudaSetDevice(device));
+    b->sm_count = prop.multiProcessorCount;
+    b->smem_optin = prop.sharedMemPerBlockOptin;
+    b->wt.resize(nprob);
+    b->jt.resize(nprob);
+    b->woff.resize(nprob);
+    b->hoff.resize(nprob);
+    size_t wtot = 0, htot = 0;
+    for (uint32_t p = 0; p < nprob; p++) {
+        default_tiles(ranks[p], m, &b->wt[p], &b->jt[p]);
+        if (problem_smem_bytes(m, ranks[p], b->wt[p], b->jt[p]) + 64 > b->smem_optin)
+            return bfail(b, NMFB_EINVAL, "m = %u with k = %u does not fit the batched engine's shared memory", m, ranks[p]);
+        b->woff[p] = wtot;
+        b->hoff[p] = htot;
+        wtot += (size_t)n * ks_of(ranks[p]);
+        htot += (size_t)m * ks_of(ranks[p]);
+    }
+    BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BTRY(b, cudaEventCreate(&b->ev0));
+    BTRY(b, cudaEventCreate(&b->ev1));
+    if (cudaMalloc(&b->dV, (size_t)n * b->ldv * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&b->dW, wtot * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&b->dH, htot * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&b->dLabels, (size_t)nprob * m * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&b->dProbs, nprob * sizeof(Problem)) != cudaSuccess ||
+        cudaMalloc(&b->dOrder, nprob * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&b->dQueue, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&b->dLabelPtrs, nprob * sizeof(uint32_t *)) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, NMFB_ENOMEM, "device allocation for the batch failed");
+    }
+    BTRY(b, cudaMemsetAsync(b->dV, 0, (size_t)n * b->ldv * sizeof(float), b->stream));
+    BTRY(b, cudaMemsetAsync(b->dW, 0, wtot * sizeof(float), b->stream));
+    BTRY(b, cudaMemsetAsync(b->dH, 0, htot * sizeof(float), b->stream));
+    std::vector<uint32_t *> lp(nprob);
+    for (uint32_t p = 0; p < nprob; p++) lp[p] = b->dLabels + (size_t)p * m;
+    BTRY(b, cudaMemcpyAsync(b->dLabelPtrs, lp.data(), nprob * sizeof(uint32_t *), cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    return NMFB_OK;
+}
+
+int nmfb_batch_destroy(nmfb_batch *b)
+{
+    if (!b) return NMFB_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    void *bufs[] = {b->dV, b->dW, b->dH, b->dLabels, b->dProbs, b->dOrder, b->dQueue, b->dLabelPtrs};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return NMFB_OK;
+}
+
+const char *nmfb_batch_last_error(const nmfb_batch *b) { return b ? b->err : "null batch"; }
+
+int nmfb_batch_set_V(nmfb_batch *b, const float *V, size_t ldv)
+{
+    if (!b || !V || ldv < b->m) return bfail(b, NMFB_EINVAL, "nmfb_batch_set_V: bad arguments");
+    BTRY(b, cudaSetDevice(b->device));
+    BTRY(b, cudaMemcpy2DAsync(b->dV, b->ldv * sizeof(float), V, ldv * sizeof(float), b->m * sizeof(float), b->n,
+                              cudaMemcpyDefault, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    b->v_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_batch_init_random(nmfb_batch *b, const uint32_t *seeds)
+{
+    if (!b || !seeds) return bfail(b, NMFB_EINVAL, "nmfb_batch_init_random: bad arguments");
+    BTRY(b, cudaSetDevice(b->device));
+    uint32_t const n = b->n, m = b->m;
+    size_t wmax = 0, hmax = 0;
+    for (uint32_t p = 0; p < b->nprob; p++) {
+        wmax = std::max(wmax, (size_t)n * ks_of(b->ranks[p]));
+        hmax = std::max(hmax, (size_t)m * ks_of(b->ranks[p]));
+    }
+    float *stage = nullptr;
+    BTRY(b, cudaMallocHost(&stage, 2 * (wmax + hmax) * sizeof(float)));
+    cudaError_t e = cudaSuccess;
+    for (uint32_t p = 0; p < b->nprob && e == cudaSuccess; p++) {
+        float *W = stage + (p & 1) * (wmax + hmax);
+        float *H = W + wmax;
+        uint32_t const k = b->ranks[p], ks = ks_of(k);
+        if (p >= 2) e = cudaStreamSynchronize(b->stream);   // the staging half of problem p-2 is free again
+        if (e != cudaSuccess) break;
+        // CPU_RANDOM initialisation (src/NMF_routines.c:206-233, 299-307):
+        // srandom(seed); W (n x k) then H (m x k), random()/RAND_MAX + FLT_MIN.
+        srandom(seeds[p]);
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t c = 0; c < ks; c++)
+                W[(size_t)i * ks + c] = (c < k) ? ((float)random()) / ((float)RAND_MAX) + FLT_MIN : 0.0f;
+        for (uint32_t j = 0; j < m; j++)
+            for (uint32_t c = 0; c < ks; c++)
+                H[(size_t)j * ks + c] = (c < k) ? ((float)random()) / ((float)RAND_MAX) + FLT_MIN : 0.0f;
+        e = cudaMemcpyAsync(b->dW + b->woff[p], W, (size_t)n * ks * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->dH + b->hoff[p], H, (size_t)m * ks * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFreeHost(stage);
+    if (e != cudaSuccess) return bfail(b, NMFB_ECUDA, "init_random: %s", cudaGetErrorString(e));
+    b->wh_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_batch_set_WH(nmfb_batch *b, uint32_t p, const float *W, size_t ldw, const float *H, size_t ldh)
+{
+    if (!b || p >= b->nprob || !W || !H) return bfail(b, NMFB_EINVAL, "nmfb_batch_set_WH: bad arguments");
+    uint32_t const k = b->ranks[p], ks = ks_of(k);
+    if (ldw < k || ldh < k) return bfail(b, NMFB_EINVAL, "nmfb_batch_set_WH: leading dimension below k");
+    BTRY(b, cudaSetDevice(b->device));
+    BTRY(b, cudaMemcpy2DAsync(b->dW + b->woff[p], ks * sizeof(float), W, ldw * sizeof(float), k * sizeof(float), b->n,
+                              cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaMemcpy2DAsync(b->dH + b->hoff[p], ks * sizeof(float), H, ldh * sizeof(float), k * sizeof(float), b->m,
+                              cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    b->wh_set = 1;
+    return NMFB_OK;
+}
+
+int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt)
+{
+    if (!b || p >= b->nprob) return bfail(b, NMFB_EINVAL, "nmfb_batch_set_tiles: bad problem");
+    if (wt < 8 || wt > 512 || (wt & 7) || jt < 4 || jt > 64 || (jt & 3))
+        return bfail(b, NMFB_EINVAL, "tile shape out of range (wt in [8, 512], multiple of 8; jt in [4, 64], multiple of 4)");
+    if (problem_smem_bytes(b->m, b->ranks[p], wt, jt) + 64 > b->smem_optin)
+        return bfail(b, NMFB_EINVAL, "tile shape does not fit shared memory");
+    b->wt[p] = wt;
+    b->jt[p] = jt;
+    return NMFB_OK;
+}
+
+int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold,
+                   uint32_t *iterations, int *converged)
+{
+    if (!b) return NMFB_EINVAL;
+    if (n_iters == 0 || niter_test_conv == 0 || stop_threshold == 0)
+        return bfail(b, NMFB_EINVAL, "nIters, niter_test_conv and stop_threshold must be positive");
+    if (!b->v_set || !b->wh_set) return bfail(b, NMFB_ESTATE, "set V and the initial factors first");
+    BTRY(b, cudaSetDevice(b->device));
+    std::vector<Problem> P(b->nprob);
+    std::vector<uint32_t> order(b->nprob);
+    size_t smem = 0;
+    for (uint32_t p = 0; p < b->nprob; p++) {
+        P[p] = make_problem(b, p);
+        order[p] = p;
+        smem = std::max(smem, problem_smem_bytes(b->m, b->ranks[p], b->wt[p], b->jt[p]));
+    }
+    // largest rank first (all problems of a sweep share n and m), stable on the index
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return b->ranks[x] > b->ranks[y]; });
+    BTRY(b, cudaMemcpyAsync(b->dProbs, P.data(), b->nprob * sizeof(Problem), cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaMemcpyAsync(b->dOrder, order.data(), b->nprob * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaMemsetAsync(b->dQueue, 0, sizeof(uint32_t), b->stream));
+    BTRY(b, cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    BTRY(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, NT, smem));
+    if (per_sm < 1) return bfail(b, NMFB_EINVAL, "batched kernel does not fit on an SM with %zu B shared memory", smem);
+    uint32_t grid = (uint32_t)per_sm * (uint32_t)b->sm_count;
+    if (grid > b->nprob) grid = b->nprob;
+    LoopArgs A{n_iters, niter_test_conv, stop_threshold};
+    BTRY(b, cudaEventRecord(b->ev0, b->stream));
+    k_batch<<<grid, NT, smem, b->stream>>>(b->dProbs, b->dOrder, b->nprob, b->dQueue, A);
+    BTRY(b, cudaGetLastError());
+    BTRY(b, cudaEventRecord(b->ev1, b->stream));
+    BTRY(b, cudaMemcpyAsync(P.data(), b->dProbs, b->nprob * sizeof(Problem), cudaMemcpyDeviceToHost, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    BTRY(b, cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    for (uint32_t p = 0; p < b->nprob; p++) {
+        if (iterations) iterations[p] = P[p].iterations;
+        if (converged) converged[p] = (int)P[p].converged;
+    }
+    return NMFB_OK;
+}
+
+int nmfb_batch_last_ms(const nmfb_batch *b, double *ms)
+{
+    if (!b || !ms) return NMFB_EINVAL;
+    *ms = b->last_ms;
+    return NMFB_OK;
+}
+
+int nmfb_batch_get_classification(nmfb_batch *b, uint32_t *labels)
+{
+    if (!b || !labels) return bfail(b, NMFB_EINVAL, "null labels");
+    BTRY(b, cudaSetDevice(b->device));
+    BTRY(b, cudaMemcpy(labels, b->dLabels, (size_t)b->nprob * b->m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return NMFB_OK;
+}
+
+int nmfb_batch_get_WH(nmfb_batch *b, uint32_t p, float *W, size_t ldw, float *H, size_t ldh)
+{
+    if (!b || p >= b->nprob) return bfail(b, NMFB_EINVAL, "bad problem index");
+    uint32_t const k = b->ranks[p], ks = ks_of(k);
+    if ((W && ldw < k) || (H && ldh < k)) return bfail(b, NMFB_EINVAL, "leading dimension below k");
+    BTRY(b, cudaSetDevice(b->device));
+    if (W)
+        BTRY(b, cudaMemcpy2D(W, ldw * sizeof(float), b->dW + b->woff[p], ks * sizeof(float), k * sizeof(float), b->n,
+                             cudaMemcpyDeviceToHost));
+    if (H)
+        BTRY(b, cudaMemcpy2D(H, ldh * sizeof(float), b->dH + b->hoff[p], ks * sizeof(float), k * sizeof(float), b->m,
+                             cudaMemcpyDeviceToHost));
+    return NMFB_OK;
+}
+
+int nmfb_batch_consensus(nmfb_batch *b, uint32_t k, uint32_t *counts, uint32_t *nruns, double *cophenetic)
+{
+    if (!b) return NMFB_EINVAL;
+    std::vector<uint32_t> sel;
+    for (uint32_t p = 0; p < b->nprob; p++)
+        if (b->ranks[p] == k) sel.push_back(p);
+    if (nruns) *nruns = (uint32_t)sel.size();
+    if (sel.empty()) return bfail(b, NMFB_EINVAL, "no problem of rank %u in the batch", k);
+    BTRY(b, cudaSetDevice(b->device));
+    uint32_t const m = b->m;
+    size_t const mm = (size_t)m * m;
+    uint32_t *dSel = nullptr, *dC = nullptr, *dCid = nullptr;
+    double *dWork = nullptr;
+    cudaError_t e = cudaMalloc(&dSel, sel.size() * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dC, mm * sizeof(uint32_t));
+    if (e == cudaSuccess && cophenetic) e = cudaMalloc(&dWork, (2 * mm + 1) * sizeof(double));
+    if (e == cudaSuccess && cophenetic) e = cudaMalloc(&dCid, 2 * (size_t)m * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dSel, sel.data(), sel.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) {
+        k_consensus<<<m, 256, 0, b->stream>>>(b->dLabelPtrs, dSel, (uint32_t)sel.size(), m, dC);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && cophenetic) {
+        k_cophenetic<<<1, 1024, 0, b->stream>>>(dC, m, (uint32_t)sel.size(), dWork, dWork + mm, dCid, dCid + m,
+                                                dWork + 2 * mm);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && counts) e = cudaMemcpyAsync(counts, dC, mm * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess && cophenetic)
+        e = cudaMemcpyAsync(cophenetic, dWork + 2 * mm, sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(dSel);
+    cudaFree(dC);
+    cudaFree(dWork);
+    cudaFree(dCid);
+    if (e != cudaSuccess) return bfail(b, NMFB_ECUDA, "consensus: %s", cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+}  // extern "C"

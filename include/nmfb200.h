@@ -161,6 +161,54 @@ int nmfb_synchronize(nmfb_ctx *ctx);
 uint64_t nmfb_launch_count(const nmfb_ctx *ctx);
 
 /* ---------------------------------------------------------------------------
+ * Batched solves: rank-selection and restart sweeps.  The reference runs one
+ * factorisation per process (nmf(), src/NMF_GPU.c:522-795; its user guide,
+ * doc/user_guide.txt.md:367, points to repeated runs and the consensus method
+ * of Brunet et al. for choosing k).  A batch runs nprob independent copies of
+ * that loop on one V (n x m), problem p with rank ranks[p] in [2, 20], all in
+ * one persistent launch, and then summarises each rank's restarts as an exact
+ * integer consensus matrix and its cophenetic correlation (FP64).
+ */
+typedef struct nmfb_batch nmfb_batch;
+
+int nmfb_batch_create(nmfb_batch **b, int device, uint32_t n, uint32_t m, uint32_t nprob, const uint32_t *ranks);
+int nmfb_batch_destroy(nmfb_batch *b);
+const char *nmfb_batch_last_error(const nmfb_batch *b);
+
+/* V: host or device pointer, n x m, leading dimension ldv >= m. */
+int nmfb_batch_set_V(nmfb_batch *b, const float *V, size_t ldv);
+
+/* CPU_RANDOM initialisation of every problem (src/NMF_routines.c:299-307),
+ * problem p from srandom(seeds[p]): the same W, H as nmfb_init_random. */
+int nmfb_batch_init_random(nmfb_batch *b, const uint32_t *seeds);
+
+/* Explicit initial factors of problem p: W (n x k), H (m x k). */
+int nmfb_batch_set_WH(nmfb_batch *b, uint32_t p, const float *W, size_t ldw, const float *H, size_t ldh);
+
+/* Tile shape of problem p: wt rows of W per update_H tile (multiple of 8,
+ * 8..512), jt columns of V per update_W tile (multiple of 4, 4..64). */
+int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt);
+
+/* Run every problem to convergence or n_iters with the reference's rules
+ * (-i n_iters, -j niter_test_conv, -t stop_threshold).  iterations[p] and
+ * converged[p] (either may be NULL) as nmfb_run reports them. */
+int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold,
+                   uint32_t *iterations, int *converged);
+
+/* Device time of the last nmfb_batch_run launch (CUDA events), milliseconds. */
+int nmfb_batch_last_ms(const nmfb_batch *b, double *ms);
+
+/* Classification of every problem's final H (nprob x m, row p = problem p). */
+int nmfb_batch_get_classification(nmfb_batch *b, uint32_t *labels);
+int nmfb_batch_get_WH(nmfb_batch *b, uint32_t p, float *W, size_t ldw, float *H, size_t ldh);
+
+/* Consensus of the problems of rank k: counts (m x m, may be NULL) = number of
+ * those runs that co-cluster each sample pair; *nruns = their number;
+ * *cophenetic (may be NULL) = cophenetic correlation of average-linkage
+ * clustering of 1 - counts / nruns. */
+int nmfb_batch_consensus(nmfb_batch *b, uint32_t k, uint32_t *counts, uint32_t *nruns, double *cophenetic);
+
+/* ---------------------------------------------------------------------------
  * update_H without any allocation.  No counterpart in the reference: it is an
  * addition of this library for callers that must not allocate device memory,
  * such as a host framework whose caching allocator already owns the HBM, a

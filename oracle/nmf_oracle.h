@@ -77,6 +77,24 @@ void oracle_dot_VWH(uint32_t n, uint32_t m, uint32_t k, const float *V, size_t l
 double oracle_kl_divergence(uint32_t n, uint32_t m, uint32_t k, const float *V, size_t ldv,
                             const float *W, size_t ldw, const float *H, size_t ldh);
 
+/* Consensus of a restart sweep (Brunet et al., PNAS 2004; cited by the
+ * reference's doc/user_guide.txt.md:367): C[a][b] = number of the nruns
+ * classification vectors (labels, nruns x m) that put samples a and b in the
+ * same class.  Exact integer counts. */
+void oracle_consensus(const uint32_t *labels, uint32_t nruns, uint32_t m, uint32_t *C);
+
+/* Cophenetic correlation of average-linkage (UPGMA) clustering of the m x m
+ * distance matrix D (symmetric, zero diagonal), FP64: merge the two active
+ * clusters at the smallest distance (lowest (a, b) slot pair on ties, a < b),
+ * the merged cluster keeps slot a with distance (|a| D[a][x] + |b| D[b][x]) /
+ * (|a| + |b|) to every other cluster x; the cophenetic distance of two samples
+ * is the merge height that joins them; result = Pearson correlation of D and
+ * the cophenetic distances over all pairs a < b. */
+double oracle_cophenetic_dist(const double *D, uint32_t m);
+
+/* The same on the consensus counts: D = 1 - C / nruns off the diagonal. */
+double oracle_cophenetic(const uint32_t *C, uint32_t m, uint32_t nruns);
+
 /* Number of OpenMP threads the oracle will use (for the benchmark record). */
 int oracle_num_threads(void);
 

@@ -54,6 +54,11 @@ def lib():
         L.oracle_difference.restype = C.c_uint64
         L.oracle_dot_VWH.argtypes = [_u32, _u32, _u32, _fp, _sz, _fp, _sz, _fp, _sz, _dp, _dp]
         L.oracle_kl_divergence.argtypes = [_u32, _u32, _u32, _fp, _sz, _fp, _sz, _fp, _sz]
+        L.oracle_consensus.argtypes = [_up, _u32, _u32, _up]
+        L.oracle_cophenetic_dist.argtypes = [_dp, _u32]
+        L.oracle_cophenetic_dist.restype = C.c_double
+        L.oracle_cophenetic.argtypes = [_up, _u32, _u32]
+        L.oracle_cophenetic.restype = C.c_double
         L.oracle_kl_divergence.restype = C.c_double
         L.oracle_num_threads.restype = C.c_int
         _lib = L
@@ -158,6 +163,25 @@ def kl_divergence(V, W, H) -> float:
     k = W.shape[1]
     return float(lib().oracle_kl_divergence(n, m, k, _p(V, C.c_float), m, _p(W, C.c_float), k,
                                             _p(H, C.c_float), k))
+
+
+def consensus(labels) -> np.ndarray:
+    """labels: nruns x m classification vectors -> m x m uint32 co-clustering counts."""
+    labels = np.ascontiguousarray(labels, np.uint32)
+    nruns, m = labels.shape
+    out = np.empty((m, m), np.uint32)
+    lib().oracle_consensus(_p(labels, C.c_uint32), nruns, m, _p(out, C.c_uint32))
+    return out
+
+
+def cophenetic(counts, nruns: int) -> float:
+    counts = np.ascontiguousarray(counts, np.uint32)
+    return float(lib().oracle_cophenetic(_p(counts, C.c_uint32), counts.shape[0], nruns))
+
+
+def cophenetic_dist(D) -> float:
+    D = np.ascontiguousarray(D, np.float64)
+    return float(lib().oracle_cophenetic_dist(_p(D, C.c_double), D.shape[0]))
 
 
 def num_threads() -> int:
