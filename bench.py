@@ -11,6 +11,12 @@ timed with CUDA events on the engine's stream; ``e2e`` = the same metric for a
 whole solve through the C ABI from pinned host buffers (V upload, CPU_RANDOM
 init, 500 iterations, W/H download).
 
+The same line carries ``plain_arm`` (the unfused FP32 arm on the same V:
+iterations/s, roofline fraction, fused speed-up) and ``sweep`` (the
+rank-selection sweep 5000 x 200, k = 2..10 x 50 restarts, as one persistent
+launch: solves/s on the device and end to end, against the same solves run
+one by one through the single-problem engine).
+
 ``--impl reference`` times the CPU restatement of the reference's loop
 (oracle/, OpenMP, all host threads) on a bounded row sample of the same
 workload, scaled to the full matrix.
@@ -42,7 +48,13 @@ WORKLOADS = {
     "C32": (60000, 5000, 32, "poisson", "60000x5000 k=32 planted Poisson(50*W0H0) counts, FP32"),
     "C64": (60000, 5000, 64, "poisson", "60000x5000 k=64 planted Poisson(50*W0H0) counts, FP32"),
     "B16": (20000, 1000, 16, "expr", "20000x1000 k=16 planted lognormal-noise matrix, 1% zeros, FP32"),
+    # profiling size of C32 for multi-pass ncu captures (V = 320 MB, still larger than L2)
+    "C32P": (16000, 5000, 32, "poisson", "16000x5000 k=32 planted Poisson(50*W0H0) counts, FP32"),
 }
+
+# Rank-selection sweep (one V, every (k, restart) pair solved to convergence).
+SWEEP = {"n": 5000, "m": 200, "true_k": 5, "ks": list(range(2, 11)), "restarts": 50, "seed": 4,
+         "desc": "5000x200 planted k=5, k=2..10 x 50 restarts, -i 2000 -j 10 -t 40"}
 
 
 def _import_package():
@@ -162,6 +174,84 @@ def cpu_port_rate(workload, budget_s=12.0, max_rows=None):
                       f"scaled by {n}/{rows} rows"}
 
 
+class L2Flush:
+    """Writes a buffer larger than L2 (126 MB) between timed steps."""
+
+    def __init__(self, dev):
+        import torch
+        self.buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB
+
+    def __call__(self, stream=None):
+        import torch
+        with torch.cuda.stream(stream) if stream is not None else _nullctx():
+            self.buf.fill_(1.0)
+
+
+class _nullctx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
+    """Config-D sweep: batched solves/s (one persistent launch per sweep, device
+    time, L2 flushed before each sweep), its end-to-end rate through the public
+    API from host memory, and the rate of the same solves run one by one
+    through the single-problem engine (a sample of seq_sample restarts per k)."""
+    import torch
+    pkg = _import_package()
+    import nmf_b200.synth as synth
+    V, _ = synth.config_d(SWEEP["seed"])
+    n, m = V.shape
+    ks, R = SWEEP["ks"], SWEEP["restarts"]
+    ranks = np.repeat(np.array(ks, np.uint32), R)
+    seeds = np.tile(np.arange(1, R + 1, dtype=np.uint32), len(ks))
+    nprob = len(ranks)
+    flush = flush or L2Flush(dev)
+    dev_ms, e2e_ms, iters = [], [], None
+    with pkg.Batch(n, m, ranks, device=dev.index or 0) as b:
+        for s in range(warmup + steps):
+            torch.cuda.synchronize()
+            flush()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.set_V(V)
+            b.init_random(seeds)
+            it, conv = b.run(2000, 10, 40)
+            b.classification()
+            coph = {k: b.consensus(k)[2] for k in ks}
+            t1 = time.perf_counter()
+            if s >= warmup:
+                dev_ms.append(b.last_ms())
+                e2e_ms.append(1e3 * (t1 - t0))
+            iters = it
+    # sequential: the same solves one at a time through the single-problem engine
+    seq_t, seq_n = 0.0, 0
+    for k in ks:
+        for r in range(1, seq_sample + 1):
+            with pkg.NMF(n, m, k, device=dev.index or 0) as e:
+                e.set_V(V)
+                e.init_random(r)
+                e.synchronize()
+                t0 = time.perf_counter()
+                e.run(2000, 10, 40)
+                seq_t += time.perf_counter() - t0
+                seq_n += 1
+    batched = nprob / (statistics.median(dev_ms) / 1e3)
+    seq = seq_n / seq_t
+    flops = float(sum(int(iters[p]) * 8.0 * n * m * int(ranks[p]) for p in range(nprob)))
+    return {"workload": SWEEP["desc"], "solves": nprob, "value": batched, "unit": "solves/s",
+            "device_ms": statistics.median(dev_ms), "e2e": {"value": nprob / (statistics.median(e2e_ms) / 1e3),
+                                                             "unit": "solves/s", "ms": statistics.median(e2e_ms)},
+            "sequential": {"value": seq, "unit": "solves/s", "sample": f"{seq_n} solves (k=2..10 x {seq_sample} seeds), "
+                                                                      "single-problem engine, host-timed"},
+            "speedup_vs_sequential": batched / seq, "tflops": flops / (statistics.median(dev_ms) / 1e3) / 1e12,
+            "mean_iterations": float(np.mean(iters)), "cophenetic": {str(k): round(v, 6) for k, v in coph.items()},
+            "l2": "256 MB buffer written before every sweep"}
+
+
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -273,6 +363,13 @@ def run_engine_arm(a, rank, world, local_rank):
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_port_rate(a.workload, budget_s=a.cpu_budget)
     e.close()
+    extras = {}
+    if rank == 0 and world == 1 and not a.no_extras:
+        extras["plain_arm"] = plain_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm)
+        extras["plain_arm"]["fused_speedup"] = value / extras["plain_arm"]["value"]
+        del V
+        torch.cuda.empty_cache()
+        extras["sweep"] = sweep_rates(dev)
     if rank != 0:
         return
     line = {"metric": "KL-NMF iterations/s", "value": value, "unit": "iters/s", "n_gpus": world,
@@ -282,7 +379,37 @@ def run_engine_arm(a, rank, world, local_rank):
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (V = %.2f GB)" % (n * m * 4 / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary()}
+    line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def plain_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, steps=2):
+    """The unfused FP32 arm on the same V and GPU: iterations/s and its roofline fraction."""
+    import torch
+    e = pkg.NMF(n, m, k, arm="plain", device=dev.index or 0)
+    try:
+        e.set_stream(stream.cuda_stream)
+        e.set_V_device(V.data_ptr(), m)
+        e.init_random(3)
+        J = a.iters_per_step
+        e.run(J, J, 2 ** 31)
+        e.synchronize()
+        e.profile(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            e.run(J, J, 2 ** 31)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        tot, cnt = e.profile_read(2)
+        e.profile(False)
+    finally:
+        e.close()
+    half_ms = tot / max(cnt, 1)
+    achieved = n * m * 4 / (half_ms / 1e3) / 1e9
+    return {"value": steps * J / (ms / 1e3), "unit": "iters/s", "update_H_ms": half_ms,
+            "roofline_frac": achieved / hbm, "note": "whole update_H (5 kernels) against n*m*4 bytes"}
 
 
 def main():
@@ -298,12 +425,29 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-arm and sweep measurements")
+    ap.add_argument("--batch-wave", type=int, default=0, metavar="K",
+                    help="profiling case of the batched kernel: one wave (2 per SM) of rank-K problems of the "
+                         "sweep matrix, 20 iterations, run twice; prints the device times")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         run_reference_arm(a, rank, world)
+        return
+    if a.batch_wave:
+        pkg = _import_package()
+        import nmf_b200.synth as synth
+        V, _ = synth.config_d(SWEEP["seed"])
+        nprob = 296
+        with pkg.Batch(V.shape[0], V.shape[1], [a.batch_wave] * nprob) as b:
+            b.set_V(V)
+            b.init_random(np.arange(1, nprob + 1, dtype=np.uint32))
+            for rep in range(2):
+                b.run(20, 20, 1 << 30)
+                print(json.dumps({"batch_wave_k": a.batch_wave, "problems": nprob, "iterations": 20,
+                                  "device_ms": b.last_ms()}), flush=True)
         return
     if world > 1:
         import datetime

@@ -173,9 +173,18 @@ __device__ __forceinline__ void stage_H(const Problem &P, float *buf, const Smem
 {
     uint32_t const q4 = L.cs / 4;
     float *sV = buf, *sW = buf + P.wt * L.cs;
-    for (uint32_t e = threadIdx.x; e < rows * q4; e += NT) {
-        uint32_t const r = e / q4, q = e - r * q4;
-        if (j0 + 4 * q < P.ldv) cp_async16(sV + r * L.cs + 4 * q, P.V + (size_t)(i0 + r) * P.ldv + j0 + 4 * q);
+    // chunk e = r * q4 + q walks in steps of NT without a division per chunk
+    uint32_t const dr = NT / q4, dq = NT - dr * q4;
+    uint32_t r = threadIdx.x / q4, q = threadIdx.x - r * q4;
+    const float *src_v = P.V + (size_t)i0 * P.ldv + j0;
+    while (r < rows) {
+        if (j0 + 4 * q < P.ldv) cp_async16(sV + r * L.cs + 4 * q, src_v + (size_t)r * P.ldv + 4 * q);
+        r += dr;
+        q += dq;
+        if (q >= q4) {
+            q -= q4;
+            r += 1;
+        }
     }
     const float *src = P.W + (size_t)i0 * KS;
     for (uint32_t e = threadIdx.x; e < rows * (KS / 4); e += NT) cp_async16(sW + 4 * e, src + 4 * e);
@@ -246,11 +255,13 @@ __device__ void update_H(const Problem &P, float *sm, const SmemLayout &L)
 __device__ __forceinline__ void stage_W(const Problem &P, float *buf, const SmemLayout &L, uint32_t i0, uint32_t rows,
                                         uint32_t j0)
 {
-    uint32_t const q4 = P.jt / 4;
-    for (uint32_t e = threadIdx.x; e < rows * q4; e += NT) {
-        uint32_t const r = e / q4, q = e - r * q4;
-        if (j0 + 4 * q < P.ldv) cp_async16(buf + r * L.vst + 4 * q, P.V + (size_t)(i0 + r) * P.ldv + j0 + 4 * q);
-    }
+    // jt is a power of two (4..64), so q4 = jt / 4 divides NT: every thread keeps
+    // one chunk column q and walks the rows in steps of NT / q4.
+    uint32_t const q4 = P.jt / 4, dr = NT / q4;
+    uint32_t const q = threadIdx.x & (q4 - 1);
+    const float *src = P.V + (size_t)i0 * P.ldv + j0 + 4 * q;
+    if (j0 + 4 * q < P.ldv)
+        for (uint32_t r = threadIdx.x / q4; r < rows; r += dr) cp_async16(buf + r * L.vst + 4 * q, src + (size_t)r * P.ldv);
 }
 
 template <int K>
@@ -871,8 +882,8 @@ int nmfb_batch_set_WH(nmfb_batch *b, uint32_t p, const float *W, size_t ldw, con
 int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt)
 {
     if (!b || p >= b->nprob) return bfail(b, NMFB_EINVAL, "nmfb_batch_set_tiles: bad problem");
-    if (wt < 8 || wt > 512 || (wt & 7) || jt < 4 || jt > 64 || (jt & 3))
-        return bfail(b, NMFB_EINVAL, "tile shape out of range (wt in [8, 512], multiple of 8; jt in [4, 64], multiple of 4)");
+    if (wt < 8 || wt > 512 || (wt & 7) || jt < 4 || jt > 64 || (jt & (jt - 1)))
+        return bfail(b, NMFB_EINVAL, "tile shape out of range (wt in [8, 512], multiple of 8; jt a power of two in [4, 64])");
     if (problem_smem_bytes(b->m, b->ranks[p], wt, jt) + 64 > b->smem_optin)
         return bfail(b, NMFB_EINVAL, "tile shape does not fit shared memory");
     b->wt[p] = wt;

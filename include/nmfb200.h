@@ -186,7 +186,7 @@ int nmfb_batch_init_random(nmfb_batch *b, const uint32_t *seeds);
 int nmfb_batch_set_WH(nmfb_batch *b, uint32_t p, const float *W, size_t ldw, const float *H, size_t ldh);
 
 /* Tile shape of problem p: wt rows of W per update_H tile (multiple of 8,
- * 8..512), jt columns of V per update_W tile (multiple of 4, 4..64). */
+ * 8..512), jt columns of V per update_W tile (a power of two, 4..64). */
 int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt);
 
 /* Run every problem to convergence or n_iters with the reference's rules
