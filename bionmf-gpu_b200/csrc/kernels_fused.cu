@@ -7,11 +7,13 @@
 //
 //   TMA      : V tile (128 x BR, FP32) into a VST-deep ring; the Y tile
 //              (BR x KP, FP32) into a YST-deep ring; X (128 x KP, FP32) once.
-//   split    : the epilogue warps turn X and each Y tile into TF32 hi + lo parts in
-//              place (hi = round-to-nearest TF32, lo = x - hi, exact) and writes
-//              the transposed Y^T hi/lo tile that MMA2 reads K-major.  (An
-//              MN-major read of the Y tile returns zeros for TF32 on sm_100a.)
-//              Only FP32 factors travel from L2: 1 + KP/128 bytes per V byte.
+//   split    : k_split_factor, once per half-iteration, writes the other
+//              factor Y as TF32 hi + lo parts (hi = round-to-nearest TF32,
+//              lo = y - hi, exact) and as the transposed hi/lo blocks that MMA2
+//              reads K-major (an MN-major read of a TF32 operand returns zeros
+//              on sm_100a); the Y producer TMA-loads all three per tile, so no
+//              warp of the fused kernel splits Y.  X (128 rows per CTA) is split
+//              in place once per CTA by the accumulator warps.
 //   MMA1     : D (TMEM, 128 x BR, FP32) = Xl Yh^T + Xh Yl^T + Xh Yh^T
 //              (tcgen05.mma kind::tf32, A and B from shared memory, K-major).
 //   epilogue : R = V / D in FP32 registers (V times an approximate reciprocal,
@@ -55,7 +57,9 @@ constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;
 struct FusedMaps {
     CUtensorMap v;       // V, box [128 x BR] (H side, no swizzle) or [32 x 128] (W side, 128B swizzle)
     CUtensorMap x;       // factor being updated (FP32, rows x KP), box rows = BO
-    CUtensorMap y;       // the other factor (FP32, rows x KP), box rows = BR
+    CUtensorMap y;       // TF32 hi part of the other factor (rows x KP), box rows = BR
+    CUtensorMap yl;      // its lo part (same layout)
+    CUtensorMap yt;      // its transposed split: per 32 rows, [hi^T (KP x 32) ; lo^T (KP x 32)]
 };
 
 struct FusedArgs {
@@ -64,6 +68,7 @@ struct FusedArgs {
     float *part;          // [split][O][KP]
     uint32_t *err;        // device error word
     const ConvState *st;
+    const float *X;       // factor being updated (O x KP), read once per CTA into TMEM
 #ifdef NMFB_FUSED_DEBUG
     float *dbg;           // block 0, tile 0: D | V | Rh | Acc (debug builds only; 128 x 64 each)
 #endif
@@ -172,16 +177,6 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
-}
-
-__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
 }
 
 __device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc, uint32_t acc)
@@ -298,17 +293,15 @@ struct Geo {
     static constexpr int NB = KP / CB;                     // column blocks
     static constexpr int ROWB = CB * 4;                    // bytes per row of a block
     static constexpr uint32_t LAYOUT = (KP == 16) ? 4u : 2u;  // SW64 : SW128
-    static constexpr int XBLK = BO * ROWB;                 // bytes of one X column block
     static constexpr int YBLK = BR * ROWB;                 // bytes of one Y column block
     static constexpr int YTBLK = KP * 128;                 // bytes of one Y^T part (32 reduction rows)
     static constexpr int YTPAIR = 2 * YTBLK;               // Y^T hi part followed by its lo part
-    static constexpr int XBYTES = BO * KP * 4;
     static constexpr int YBYTES = BR * KP * 4;
     static constexpr int VBYTES = BO * BR * 4;
     static constexpr int YSTAGE = 2 * YBYTES;              // Yh (TMA target, split in place) | Yl
     static constexpr int YTSTAGE = 2 * YBYTES;             // YTh | YTl
     static constexpr int YST = 3;
-    static constexpr int FIXED = 1024 + 2 * XBYTES + 512;
+    static constexpr int FIXED = 1024 + 512;
     static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YST * (YSTAGE + YTSTAGE)) / VBYTES;
     static constexpr int VST = VAVAIL > 6 ? 6 : VAVAIL;    // V ring depth (HBM stream)
     static constexpr int SMEM = FIXED + YST * (YSTAGE + YTSTAGE) + VST * VBYTES;
@@ -318,60 +311,46 @@ struct Geo {
     static constexpr int NTHR = (4 + NR + 4) * 32;
     static constexpr uint32_t ACC = 2 * KP;                // TMEM columns of one per-tile accumulator
     static constexpr uint32_t DB0 = 2 * ACC;               // first D buffer column
+    static constexpr uint32_t NDB = (KP == 16) ? 3 : 2;    // D buffers (MMA1 runs NDB tiles ahead)
+    static constexpr uint32_t XC0 = DB0 + NDB * 2 * BR;    // X hi at XC0, X lo at XC0 + KP
+    static_assert(XC0 + 2 * KP <= 512, "TMEM columns exceeded");
 };
 
 // TMEM columns: per-tile accumulators Acc[b] at b*2KP (2KP columns: the Rh Y^T_hi
 // + Rl Y^T_hi sum and the Rh Y^T_lo part side by side), D[b] (later Rh[b]) at
-// 4KP + b*2*BR, Rl[b] at 4KP + b*2*BR + BR, b < NDB.  Three D buffers let MMA1
-// run three tiles ahead of the R warps (KP=32: 128 + 3*128 = 512 columns).
-constexpr uint32_t NDB = 3;
+// 4KP + b*2*BR, Rl[b] at 4KP + b*2*BR + BR, b < NDB; then the CTA's 128 rows of
+// X as TF32 hi (KP columns) and lo (KP columns), the A operand of MMA1 for every
+// tile (so MMA1 reads only Y from shared memory).
 
-// Byte offset of element (row r, column c) in a K-major tile of G::CB-float
-// column blocks with 128B (CB = 32) or 64B (CB = 16) swizzle (the TMA layout).
-template <int KP>
-__device__ __forceinline__ uint32_t kmaj_off(uint32_t r, uint32_t c, uint32_t blk_bytes)
+// Split a factor Y (rows x kp, FP32, padding columns zero) for the fused
+// kernel's TMA loads: hi = TF32(y) (round to nearest), lo = y - hi (exact),
+// both rows x kp; and per block of 32 rows the transposed hi block (kp rows of
+// 32 floats) followed by the transposed lo block, rows past the end zero.
+// One CTA per 32-row block; the transpose goes through shared memory.
+__global__ void __launch_bounds__(256) k_split_factor(const float *__restrict__ Y, uint32_t rows, uint32_t kp,
+                                                      float *__restrict__ hi, float *__restrict__ lo,
+                                                      float *__restrict__ T, const ConvState *st)
 {
-    using G = Geo<KP>;
-    uint32_t const b = c / G::CB, cc = c % G::CB;
-    uint32_t const chunk = cc >> 2;
-    uint32_t const sw = (G::CB == 32) ? (r & 7) : ((r >> 1) & 3);
-    return b * blk_bytes + r * G::ROWB + ((chunk ^ sw) << 4) + (cc & 3) * 4;
-}
-
-// Split rows [0, rows) of a K-major FP32 tile in place into TF32 hi (same
-// place) and lo (at `lo`, same layout); when `t_hi` is given, also write the
-// transpose (K-major over the rows, 128B swizzle; for each block of 32 rows
-// the hi part, KP x 128 B, directly followed by the lo part, so that one MMA
-// with N = 2 KP reads both).
-template <int KP>
-__device__ __forceinline__ void split_tile(unsigned char *hi, unsigned char *lo, unsigned char *t_hi,
-                                           uint32_t rows, uint32_t blk_bytes, uint32_t tid, uint32_t nthr)
-{
-    for (uint32_t q = tid; q < rows * (KP / 4); q += nthr) {
-        uint32_t const r = q / (KP / 4), c = (q % (KP / 4)) * 4;
-        {
-            uint32_t const off = kmaj_off<KP>(r, c, blk_bytes);
-            float4 const x = *reinterpret_cast<const float4 *>(hi + off);
-            float4 h, l;
-            h.x = tf32_rna(x.x); l.x = x.x - h.x;
-            h.y = tf32_rna(x.y); l.y = x.y - h.y;
-            h.z = tf32_rna(x.z); l.z = x.z - h.z;
-            h.w = tf32_rna(x.w); l.w = x.w - h.w;
-            *reinterpret_cast<float4 *>(hi + off) = h;
-            *reinterpret_cast<float4 *>(lo + off) = l;
-            if (t_hi) {
-                // Y^T: per block of 32 rows, the hi part (KP rows of 128 B) followed by the lo part.
-                uint32_t const rb = r >> 5, rr = r & 31;
-                float hv[4] = {h.x, h.y, h.z, h.w}, lv[4] = {l.x, l.y, l.z, l.w};
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    uint32_t const cc = c + i;
-                    uint32_t const toff = rb * (2 * KP * 128) + cc * 128 + (((rr >> 2) ^ (cc & 7)) << 4) + (rr & 3) * 4;
-                    *reinterpret_cast<float *>(t_hi + toff) = hv[i];
-                    *reinterpret_cast<float *>(t_hi + toff + KP * 128) = lv[i];
-                }
-            }
+    if (st && *(volatile const uint32_t *)&st->converged) return;
+    __shared__ float th[32][65], tl[32][65];
+    uint32_t const r0 = blockIdx.x * 32;
+    for (uint32_t e = threadIdx.x; e < 32 * kp; e += blockDim.x) {
+        uint32_t const r = e / kp, c = e % kp;
+        bool const in = r0 + r < rows;
+        float const y = in ? Y[(size_t)(r0 + r) * kp + c] : 0.0f;
+        float const h = tf32_rna(y), l = y - h;
+        if (in) {
+            hi[(size_t)(r0 + r) * kp + c] = h;
+            lo[(size_t)(r0 + r) * kp + c] = l;
         }
+        th[r][c] = h;
+        tl[r][c] = l;
+    }
+    __syncthreads();
+    float *dst = T + (size_t)blockIdx.x * 2 * kp * 32;
+    for (uint32_t e = threadIdx.x; e < 2 * kp * 32; e += blockDim.x) {
+        uint32_t const row = e / 32, rr = e % 32;
+        dst[e] = row < kp ? th[rr][row] : tl[rr][row - kp];
     }
 }
 
@@ -394,23 +373,19 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     extern __shared__ unsigned char smem_raw[];
     uint32_t const base_u32 = (smem_u32(smem_raw) + 1023u) & ~1023u;
     unsigned char *const base = smem_raw + (base_u32 - smem_u32(smem_raw));
-    unsigned char *const sXh = base;                                // TMA target, split in place
-    unsigned char *const sXl = base + G::XBYTES;
-    unsigned char *const sY = base + 2 * G::XBYTES;                 // [YST][Yh | Yl]
+    unsigned char *const sY = base;                                 // [YST][Yh | Yl]
     unsigned char *const sYT = sY + G::YST * G::YSTAGE;             // [YST][YTh | YTl]
     unsigned char *const sV = sYT + G::YST * G::YTSTAGE;            // [VST][VBYTES]
     uint64_t *const bars = reinterpret_cast<uint64_t *>(sV + G::VST * G::VBYTES);
     uint64_t *const vfull = bars;                   // [VST]  TMA -> epilogue
     uint64_t *const vempty = vfull + G::VST;        // [VST]  epilogue -> V producer
-    uint64_t *const yraw = vempty + G::VST;         // [YST]  TMA -> splitter
-    uint64_t *const yready = yraw + G::YST;         // [YST]  epilogue split -> MMA1 / MMA2
-    uint64_t *const yempty = yready + G::YST;       // [YST]  MMA1 commit -> Y producer
+    uint64_t *const yfull = vempty + G::VST;        // [YST]  TMA (Yh, Yl, Y^T) -> MMA1 / MMA2
+    uint64_t *const yempty = yfull + G::YST;        // [YST]  MMA2 commit -> Y producer
     uint64_t *const dfull = yempty + G::YST;        // [NDB]  MMA1 commit -> R warps
-    uint64_t *const rfull = dfull + NDB;            // [NDB]  R warps -> MMA2
-    uint64_t *const accrdy = rfull + NDB;           // [2]    MMA2 commit -> accumulator warps
+    uint64_t *const rfull = dfull + G::NDB;         // [NDB]  R warps -> MMA2
+    uint64_t *const accrdy = rfull + G::NDB;        // [2]    MMA2 commit -> accumulator warps
     uint64_t *const accfree = accrdy + 2;           // [2]    accumulator warps -> MMA2
-    uint64_t *const xraw = accfree + 2;             // [1]    TMA -> splitter
-    uint64_t *const xready = xraw + 1;              // [1]    epilogue split -> MMA1
+    uint64_t *const xready = accfree + 2;           // [1]    X split into TMEM -> MMA1
     uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xready + 1);
     volatile uint32_t *const abort_flag = tmem_slot + 1;
 
@@ -446,11 +421,10 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             mbar_init(&vempty[s], NR);
         }
         for (int s = 0; s < G::YST; s++) {
-            mbar_init(&yraw[s], 1);
-            mbar_init(&yready[s], 4);
+            mbar_init(&yfull[s], 1);
             mbar_init(&yempty[s], 1);
         }
-        for (uint32_t b = 0; b < NDB; b++) {
+        for (uint32_t b = 0; b < G::NDB; b++) {
             mbar_init(&dfull[b], 1);
             mbar_init(&rfull[b], NR);
         }
@@ -458,7 +432,6 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             mbar_init(&accrdy[b], 1);
             mbar_init(&accfree[b], 4);
         }
-        mbar_init(xraw, 1);
         mbar_init(xready, 4);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -499,11 +472,9 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             }
         }
     } else if (warp == 2) {
-        // ------------------------------------------------------------ X / Y producer
+        // ------------------------------------------------------------ Y producer
         if (lane == 0) {
             uint64_t const pol = policy_evict_last();
-            mbar_expect_tx(xraw, G::XBYTES);
-            for (int b = 0; b < G::NB; b++) tma_load_2d(sXh + b * G::XBLK, &maps.x, xraw, b * G::CB, (int)o0, pol);
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::YST;
                 if (t >= (uint32_t)G::YST &&
@@ -512,8 +483,13 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                 unsigned char *syh = sY + s * G::YSTAGE;
                 int const r0 = (int)((t_begin + t) * BR);
                 DBG_TS(1, t);
-                mbar_expect_tx(&yraw[s], G::YBYTES);
-                for (int b = 0; b < G::NB; b++) tma_load_2d(syh + b * G::YBLK, &maps.y, &yraw[s], b * G::CB, r0, pol);
+                mbar_expect_tx(&yfull[s], (NTERMS == 3 ? 2 : 1) * G::YBYTES + G::YTSTAGE);
+                for (int b = 0; b < G::NB; b++) tma_load_2d(syh + b * G::YBLK, &maps.y, &yfull[s], b * G::CB, r0, pol);
+                if (NTERMS == 3)
+                    for (int b = 0; b < G::NB; b++)
+                        tma_load_2d(syh + G::YBYTES + b * G::YBLK, &maps.yl, &yfull[s], b * G::CB, r0, pol);
+                // Y^T: the BR / 32 row blocks of this tile, 2 KP rows of 128 B each
+                tma_load_2d(sYT + s * G::YTSTAGE, &maps.yt, &yfull[s], 0, (r0 / 32) * 2 * KP, pol);
             }
         }
     } else if (warp == 1) {
@@ -521,8 +497,9 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         // Two issue queues, polled without blocking (nanosleep back-off):
         //   MMA2(n2): needs the R warps' R(n2) and, for n2 >= 2, the accumulator
         //             warps to have read Acc[n2 % 2] of tile n2-2;
-        //   MMA1(n1): needs the split Y(n1) and a free D buffer (MMA2(n1-NDB)
-        //             issued, i.e. n1 < n2 + NDB).
+        //   MMA1(n1): needs Y(n1) loaded and a free D buffer (MMA2(n1-NDB)
+        //             issued, i.e. n1 < n2 + NDB); A = X from TMEM.
+        // The Y stage of tile t is released when MMA2(t), the last reader, completes.
         if (lane == 0) {
             constexpr uint32_t IDESC1 = idesc_tf32(BO, BR, 0);
             constexpr uint32_t IDESC2 = idesc_tf32(BO, KP, 0);
@@ -530,8 +507,6 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             // Shared-memory descriptors are built once; a k-step or stage offset is
             // added to the start-address field (16-byte units, no carry out of it:
             // every operand lies below 256 KB).
-            uint64_t const dXh = smem_desc(smem_u32(sXh), 16, 8 * G::ROWB, G::LAYOUT);
-            uint64_t const dXl = smem_desc(smem_u32(sXl), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dYT0 = smem_desc(smem_u32(sYT), 16, 1024, 2u);
             bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u);
@@ -540,10 +515,10 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             unsigned long long last = globaltimer();
             while (ok && n2 < T) {
                 bool progressed = false;
-                if (n2 < n1 && mbar_test(&rfull[n2 % NDB], (n2 / NDB) & 1) &&
+                if (n2 < n1 && mbar_test(&rfull[n2 % G::NDB], (n2 / G::NDB) & 1) &&
                     (n2 < 2 || mbar_test(&accfree[n2 & 1], ((n2 >> 1) - 1) & 1))) {
                     tc_fence_after();
-                    uint32_t const sp = n2 % G::YST, bp = n2 & 1, db = n2 % NDB;
+                    uint32_t const sp = n2 % G::YST, bp = n2 & 1, db = n2 % G::NDB;
                     uint64_t const dYT = dYT0 + ((sp * G::YTSTAGE) >> 4);
                     uint32_t const rh = tmem + DBUF0 + db * 2 * BR;
                     uint32_t const rl = rh + BR;
@@ -564,13 +539,14 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                         }
                     }
                     tc_commit(&accrdy[bp]);
+                    tc_commit(&yempty[sp]);
                     DBG_TS(3, n2);
                     n2++;
                     progressed = true;
                 }
-                if (n1 < T && n1 < n2 + NDB && mbar_test(&yready[n1 % G::YST], (n1 / G::YST) & 1)) {
+                if (n1 < T && n1 < n2 + G::NDB && mbar_test(&yfull[n1 % G::YST], (n1 / G::YST) & 1)) {
                     tc_fence_after();
-                    uint32_t const s = n1 % G::YST, db = n1 % NDB;
+                    uint32_t const s = n1 % G::YST, db = n1 % G::NDB;
                     uint64_t const dYh = dY0 + ((s * G::YSTAGE) >> 4);
                     uint64_t const dYl = dYh + (G::YBYTES >> 4);
                     uint32_t const dcol = tmem + DBUF0 + db * 2 * BR;
@@ -578,18 +554,16 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
 #pragma unroll
                     for (int tt = 0; tt < NTERMS; tt++) {
                         int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
-                        uint64_t const xa = (term == 2) ? dXl : dXh;
+                        uint32_t const xa = tmem + G::XC0 + ((term == 2) ? KP : 0);
                         uint64_t const yb = (term == 1) ? dYl : dYh;
 #pragma unroll
                         for (int ks = 0; ks < KP / 8; ks++) {
                             constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
-                            uint32_t const oa = ((ks / KPB) * G::XBLK + (ks % KPB) * 32) >> 4;
                             uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
-                            mma_ss(dcol, xa + oa, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
+                            mma_ts(dcol, xa + ks * 8, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
                         }
                     }
                     tc_commit(&dfull[db]);
-                    tc_commit(&yempty[s]);
                     DBG_TS(2, n1);
                     n1++;
                     progressed = true;
@@ -614,10 +588,10 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         uint32_t const row = quad * 32 + lane;        // TMEM lane = output row within the block
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
         for (uint32_t t = 0; t < T; t++) {
-            uint32_t const s = t % G::VST, b = t % NDB;
+            uint32_t const s = t % G::VST, b = t % G::NDB;
             if (warp == 4 && lane == 0) DBG_TS(4, t);
             DBG_PH(0, t);
-            if (!mbar_wait(&dfull[b], (t / NDB) & 1, abort_flag, args.err, 6u)) break;
+            if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 6u)) break;
             DBG_PH(1, t);
             if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) break;
             tc_fence_after();
@@ -704,34 +678,40 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     } else if (warp >= 4 + NR) {
         // ------------------------------------------------------------ accumulator warps
         // Warp 4+NR+q owns TMEM lanes 32q..32q+31: sums the per-tile Acc into FP32
-        // registers, and (all four together) splits X and the Y tiles.
+        // registers, and (all four together) splits X once.
         uint32_t const quad = warp & 3;
         uint32_t const row = quad * 32 + lane;
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
-        uint32_t const atid = (warp - 4 - NR) * 32 + lane;  // 0..127, for the cooperative splits
         float sum[KP];
 #pragma unroll
         for (int c = 0; c < KP; c++) sum[c] = 0.0f;
-        // Split Y(ty) (already in shared memory) into TF32 hi/lo and its transpose.
-        auto split_y = [&](uint32_t ty) -> bool {
-            uint32_t const s = ty % G::YST;
-            if (!mbar_wait(&yraw[s], (ty / G::YST) & 1, abort_flag, args.err, 11u)) return false;
-            unsigned char *syh = sY + s * G::YSTAGE;
-            unsigned char *syth = sYT + s * G::YTSTAGE;
-            split_tile<KP>(syh, syh + G::YBYTES, syth, BR, G::YBLK, atid, 128);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&yready[s]);
-            return true;
-        };
-        bool ok = mbar_wait(xraw, 0, abort_flag, args.err, 10u);
-        if (ok) {
-            split_tile<KP>(sXh, sXl, nullptr, BO, G::XBLK, atid, 128);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bool ok = true;
+        {   // this thread's row of X, split into TF32 hi / lo, into TMEM lanes = rows
+            uint32_t const o = o0 + row;
+            const float *xr = args.X + (size_t)o * KP;
+#pragma unroll
+            for (int c0 = 0; c0 < KP; c0 += 16) {
+                uint32_t h[32], l[32];
+#pragma unroll
+                for (int c = 0; c < 16; c += 4) {
+                    float4 const x = (o < args.O) ? *reinterpret_cast<const float4 *>(xr + c0 + c)
+                                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    float const xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        float const hv = tf32_rna(xs[i]);
+                        h[c + i] = __float_as_uint(hv);
+                        l[c + i] = __float_as_uint(xs[i] - hv);
+                    }
+                }
+                tmem_st16(lane_addr + G::XC0 + c0, h);
+                tmem_st16(lane_addr + G::XC0 + KP + c0, l);
+            }
+            tmem_wait_st();
+            tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(xready);
         }
-        for (uint32_t ty = 0; ok && ty < (uint32_t)G::YST && ty < T; ty++) ok = split_y(ty);
         for (uint32_t t = 0; ok && t < T; t++) {
             uint32_t const bp = t & 1;
             if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
@@ -752,8 +732,6 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&accfree[bp]);
             if (warp == 4 + NR && lane == 0) DBG_TS(7, t);
-            // MMA2(t) has completed, so its Y^T stage (t % YST) is free: prepare Y(t + YST).
-            if (t + G::YST < T && !split_y(t + G::YST)) { ok = false; break; }
 #ifdef NMFB_FUSED_DEBUG
             if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[1024 + (warp - 4 - NR) * 64 + t] = globaltimer() - ts0;
 #endif
@@ -821,6 +799,7 @@ int encode_2d(nmfb_ctx *ctx, CUtensorMap *map, const float *base, uint64_t inner
 struct FusedPlan {
     FusedMaps mapsH, mapsW;  // update_H (HSIDE) and update_W
     uint32_t *dErr;
+    float *dSplitW, *dSplitH;  // hi | lo | transposed blocks of W and of H (k_split_factor)
 #ifdef NMFB_FUSED_DEBUG
     float *dDbg;
 #endif
@@ -837,12 +816,22 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
     uint32_t const R = HSIDE ? ctx->n : ctx->m;
     uint32_t const oblocks = (O + BO - 1) / BO;
     uint32_t const T = (R + BR - 1) / BR;
-    // Splits of the reduction so that the grid fills the GPU a few times over.
-    uint32_t want = (4u * (uint32_t)ctx->sm_count + oblocks - 1) / oblocks;
-    if (want < 1) want = 1;
-    if (want > NMFB_MAX_SPLIT) want = NMFB_MAX_SPLIT;
-    uint32_t tps = (T + want - 1) / want;
-    if (tps < 4) tps = T < 4 ? T : 4;
+    // Splits of the reduction: one CTA per SM at a time, so the launch takes
+    // ceil(CTAs / SMs) waves of (tiles per split + pipeline fill) tile times;
+    // pick the split count that minimises that (fill ~ 3 tiles: TMEM
+    // allocation, X load and split, first MMA1, partial write).
+    uint32_t tps = T, best = 0xffffffffu;
+    for (uint32_t want = 1; want <= NMFB_MAX_SPLIT && want <= T; want++) {
+        uint32_t const t_ps = (T + want - 1) / want;
+        uint32_t const ns = (T + t_ps - 1) / t_ps;
+        if ((size_t)ns * O * KP > ctx->part_items) break;
+        uint32_t const waves = (oblocks * ns + (uint32_t)ctx->sm_count - 1) / (uint32_t)ctx->sm_count;
+        uint32_t const cost = waves * (t_ps + 3);
+        if (cost < best) {
+            best = cost;
+            tps = t_ps;
+        }
+    }
     uint32_t const nsplit = (T + tps - 1) / tps;
     if ((size_t)nsplit * O * KP > ctx->part_items)
         return nmfb_fail(ctx, NMFB_EINVAL, "fused: partial buffer too small (%u splits)", nsplit);
@@ -854,6 +843,7 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
     args.part = ctx->dPart;
     args.err = plan->dErr;
     args.st = ctx->dState;
+    args.X = HSIDE ? ctx->dH : ctx->dW;
 #ifdef NMFB_FUSED_DEBUG
     args.dbg = plan->dDbg;
 #endif
@@ -891,6 +881,13 @@ int fused_half(nmfb_ctx *ctx, bool is_H, int adjust)
     int rc = nmfb_prof_begin(ctx, whole);
     if (rc) return rc;
     if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
+    {
+        float *sp = is_H ? plan->dSplitW : plan->dSplitH;
+        size_t const part = (size_t)yrows * ctx->kp;
+        k_split_factor<<<(yrows + 31) / 32, 256, 0, ctx->stream>>>(Y, yrows, ctx->kp, sp, sp + part, sp + 2 * part,
+                                                                   ctx->dState);
+        NMFB_LAUNCH_CHECK(ctx);
+    }
     int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH) : dispatch<false>(ctx, plan->mapsW);
     if (nsplit < 0) return nsplit;
     rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust);
@@ -933,16 +930,31 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
     uint64_t const vrow = ctx->ldv * sizeof(float), frow = (uint64_t)kp * sizeof(float);
     uint32_t const br = (kp >= 64) ? 32 : 64;
+    // Split copies of W and H: hi (rows x kp) | lo (rows x kp) | transposed blocks
+    // (ceil(rows / 32) blocks of 2 kp x 32 floats).
+    size_t const wsz = (size_t)ctx->n * kp, hsz = (size_t)ctx->m * kp;
+    uint32_t const wblk = (ctx->n + 31) / 32, hblk = (ctx->m + 31) / 32;
+    e = cudaMalloc((void **)&plan->dSplitW, (2 * wsz + (size_t)wblk * 64 * kp) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&plan->dSplitH, (2 * hsz + (size_t)hblk * 64 * kp) * sizeof(float));
+    if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused split buffers: %s", cudaGetErrorString(e));
     // update_H: X = H (rows m), Y = W (rows n); V tile [br rows of V][128 cols].
     FusedMaps &mh = plan->mapsH;
     if ((rc = encode_2d(ctx, &mh.v, ctx->dV, ctx->m, ctx->n, vrow, BO, br, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
     if ((rc = encode_2d(ctx, &mh.x, ctx->dH, kp, ctx->m, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.y, ctx->dW, kp, ctx->n, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.y, plan->dSplitW, kp, ctx->n, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.yl, plan->dSplitW + wsz, kp, ctx->n, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mh.yt, plan->dSplitW + 2 * wsz, 32, (uint64_t)wblk * 2 * kp, 128, 32, 2 * kp * (br / 32),
+                        CU_TENSOR_MAP_SWIZZLE_128B)))
+        return rc;
     // update_W: X = W (rows n), Y = H (rows m); V tile [128 rows][32 cols] x (br/32), 128B swizzle.
     FusedMaps &mw = plan->mapsW;
     if ((rc = encode_2d(ctx, &mw.v, ctx->dV, ctx->m, ctx->n, vrow, 32, BO, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
     if ((rc = encode_2d(ctx, &mw.x, ctx->dW, kp, ctx->n, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.y, ctx->dH, kp, ctx->m, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.y, plan->dSplitH, kp, ctx->m, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.yl, plan->dSplitH + hsz, kp, ctx->m, frow, cb, br, fsw))) return rc;
+    if ((rc = encode_2d(ctx, &mw.yt, plan->dSplitH + 2 * hsz, 32, (uint64_t)hblk * 2 * kp, 128, 32, 2 * kp * (br / 32),
+                        CU_TENSOR_MAP_SWIZZLE_128B)))
+        return rc;
     return NMFB_OK;
 }
 
@@ -951,6 +963,8 @@ int nmfb_fused_release(nmfb_ctx *ctx)
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
     if (!plan) return NMFB_OK;
     if (plan->dErr) cudaFree(plan->dErr);
+    if (plan->dSplitW) cudaFree(plan->dSplitW);
+    if (plan->dSplitH) cudaFree(plan->dSplitH);
     free(plan);
     ctx->tmaps = nullptr;
     return NMFB_OK;

@@ -181,7 +181,7 @@ int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, 
     if ((rc = dev_alloc(ctx, &ctx->dAccH, kp, "accH"))) return rc;
     // Split-reduction partials: both arms size their splits so that
     // nsplit * rows <= 4*SMs*128 + 2*rows + 128 (see the split planners).
-    ctx->part_items = ((size_t)512 * ctx->sm_count + 2 * maxr + 256) * kp;
+    ctx->part_items = ((size_t)512 * ctx->sm_count + 4 * maxr + 256) * kp;
     if ((rc = dev_alloc(ctx, &ctx->dPart, ctx->part_items, "partials"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dColPart, (size_t)2 * 1024 * kp, "colsum partials"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dTickets, 16, "tickets"))) return rc;
