@@ -418,7 +418,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--arm", default="fused", choices=["fused", "plain", "fused_tf32"])
+    ap.add_argument("--arm", default="fused", choices=["fused", "plain", "fused_tf32", "bf16", "split_bf16", "bf16x3"])
     ap.add_argument("--workload", default="C32", choices=list(WORKLOADS))
     ap.add_argument("--iters-per-step", type=int, default=10)
     ap.add_argument("--e2e-iters", type=int, default=500)

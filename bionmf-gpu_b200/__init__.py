@@ -33,7 +33,11 @@ HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "nmfb200.h")
 ARM_FUSED = 0
 ARM_PLAIN = 1
 ARM_FUSED_TF32 = 2
-ARMS = {"fused": ARM_FUSED, "plain": ARM_PLAIN, "fused_tf32": ARM_FUSED_TF32}
+ARM_BF16 = 3
+ARM_SPLIT_BF16 = 4
+ARM_BF16X3 = 5
+ARMS = {"fused": ARM_FUSED, "plain": ARM_PLAIN, "fused_tf32": ARM_FUSED_TF32, "bf16": ARM_BF16,
+        "split_bf16": ARM_SPLIT_BF16, "bf16x3": ARM_BF16X3}
 
 NMFB_OK = 0
 _ERRNAMES = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENODEV", -5: "ESTATE", -6: "ETIMEOUT", -7: "ETOOBIG"}

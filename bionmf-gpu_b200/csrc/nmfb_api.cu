@@ -50,6 +50,7 @@ void free_all(nmfb_ctx *ctx)
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->hState) cudaFreeHost(ctx->hState);
+    nmfb_bf16_release(ctx);
     nmfb_fused_release(ctx);
     for (int c = 0; c < 4; c++) {
         if (!ctx->prof_ev[c]) continue;
@@ -95,12 +96,14 @@ int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, 
 int do_update_H(nmfb_ctx *ctx, int adjust)
 {
     if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_H(ctx, adjust);
+    if (ctx->arm >= NMFB_ARM_BF16) return nmfb_bf16_update_H(ctx, adjust);
     return nmfb_fused_update_H(ctx, adjust);
 }
 
 int do_update_W(nmfb_ctx *ctx, int adjust)
 {
     if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_W(ctx, adjust);
+    if (ctx->arm >= NMFB_ARM_BF16) return nmfb_bf16_update_W(ctx, adjust);
     return nmfb_fused_update_W(ctx, adjust);
 }
 
@@ -150,7 +153,7 @@ int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, 
         return nmfb_fail(ctx, NMFB_EINVAL,
                          "invalid factorization rank: K=%u. It must not be greater than any of matrix dimensions.", k);
     if (k > 256) return nmfb_fail(ctx, NMFB_EINVAL, "factorization rank K=%u exceeds the supported maximum of 256", k);
-    if (arm != NMFB_ARM_FUSED && arm != NMFB_ARM_PLAIN && arm != NMFB_ARM_FUSED_TF32)
+    if (arm < NMFB_ARM_FUSED || arm > NMFB_ARM_BF16X3)
         return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
@@ -205,7 +208,7 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (arm != NMFB_ARM_FUSED && arm != NMFB_ARM_PLAIN && arm != NMFB_ARM_FUSED_TF32)
+    if (arm < NMFB_ARM_FUSED || arm > NMFB_ARM_BF16X3)
         return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
     if (arm == NMFB_ARM_PLAIN) {
         if (!ctx->dWH && (rc = dev_alloc(ctx, &ctx->dWH, (size_t)ctx->n * ctx->ldv, "WH"))) return rc;
@@ -215,6 +218,7 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
     if (ctx->kp > 64)
         return nmfb_fail(ctx, NMFB_EINVAL, "the fused arms support ranks up to 64 (k=%u); use NMFB_ARM_PLAIN", ctx->k);
     if ((rc = nmfb_fused_prepare(ctx))) return rc;
+    if (arm >= NMFB_ARM_BF16 && (rc = nmfb_bf16_prepare(ctx))) return rc;
     ctx->arm = arm;
     return NMFB_OK;
 }

@@ -46,6 +46,7 @@ struct nmfb_ctx {
 
     int sm_count;
     void *tmaps;           // fused-arm tensor maps (host copy), see kernels_fused.cu
+    void *bplan;           // bf16-arm plan, see kernels_bf16.cu
 
     // Convergence test state.
     uint32_t *dLabels;     // m
@@ -111,6 +112,13 @@ int nmfb_fused_release(nmfb_ctx *ctx);
 int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust);
 int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code);
+uint32_t *nmfb_fused_err_word(nmfb_ctx *ctx);
+
+// ---- kernels_bf16.cu ------------------------------------------------------
+int nmfb_bf16_prepare(nmfb_ctx *ctx);
+int nmfb_bf16_release(nmfb_ctx *ctx);
+int nmfb_bf16_update_H(nmfb_ctx *ctx, int adjust);
+int nmfb_bf16_update_W(nmfb_ctx *ctx, int adjust);
 
 // Max number of reduction splits used by any arm (sizes dPart).
 #define NMFB_MAX_SPLIT 64

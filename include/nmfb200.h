@@ -43,6 +43,9 @@ extern "C" {
 #define NMFB_ARM_FUSED 0  /* fused half-iteration, tcgen05 3xTF32 (FP32-accurate) */
 #define NMFB_ARM_PLAIN 1  /* unfused FP32 SIMT kernels mirroring the reference's 5 steps */
 #define NMFB_ARM_FUSED_TF32 2 /* fused, 1xTF32 denominator (reduced precision) */
+#define NMFB_ARM_BF16 3       /* fused, BF16 operands, FP32 accumulation (reduced precision) */
+#define NMFB_ARM_SPLIT_BF16 4 /* fused, split-BF16 WH denominator (3 products), one BF16 product in the second contraction */
+#define NMFB_ARM_BF16X3 5     /* fused, split-BF16 (3 products) in both contractions (FP32-class) */
 
 typedef struct nmfb_ctx nmfb_ctx;
 
