@@ -50,6 +50,8 @@ WORKLOADS = {
     "B16": (20000, 1000, 16, "expr", "20000x1000 k=16 planted lognormal-noise matrix, 1% zeros, FP32"),
     # profiling size of C32 for multi-pass ncu captures (V = 320 MB, still larger than L2)
     "C32P": (16000, 5000, 32, "poisson", "16000x5000 k=32 planted Poisson(50*W0H0) counts, FP32"),
+    # blockwise (out-of-core) mode: V in host memory, streamed in row blocks
+    "S32": (250000, 20000, 32, "poisson", "250000x20000 k=32 planted Poisson counts, FP32, V in host memory (20 GB)"),
 }
 
 # Rank-selection sweep (one V, every (k, restart) pair solved to convergence).
@@ -252,6 +254,53 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
             "l2": "256 MB buffer written before every sweep"}
 
 
+def stream_rates(dev, iters=3):
+    """Blockwise mode on the S32 workload: iterations/s with V read from
+    page-locked host memory every half-iteration, the achieved host-to-device
+    rate (2 n m 4 bytes per iteration) and the measured copy peak of the link
+    (one 1 GiB pinned host-to-device copy)."""
+    import torch
+    pkg = _import_package()
+    n, m, k, _, desc = WORKLOADS["S32"]
+    Vd = make_V("S32", dev)
+    Vh = torch.empty((n, m), dtype=torch.float32, pin_memory=True)
+    Vh.copy_(Vd)
+    del Vd
+    torch.cuda.empty_cache()
+    # link peak: 1 GiB pinned H2D copy, best of 3
+    src = Vh.view(-1)[: 1 << 28]
+    dst = torch.empty_like(src, device=dev)
+    peak = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        peak = max(peak, src.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del dst
+    stream = torch.cuda.Stream(device=dev)
+    with pkg.NMF(n, m, k, device=dev.index or 0, stream_rows=0) as e:
+        e.set_stream(stream.cuda_stream)
+        e.set_V(Vh.numpy())
+        e.init_random(3)
+        e.run(1, 1, 2 ** 31)
+        e.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.run(iters, iters, 2 ** 31)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+    rate = iters / (ms / 1e3)
+    h2d = 2.0 * n * m * 4 * iters / (ms / 1e3) / 1e9
+    return {"workload": desc, "value": rate, "unit": "iters/s", "h2d_gbs": h2d, "h2d_peak_gbs": peak,
+            "frac_of_link": h2d / peak, "bytes_per_iteration": 2 * n * m * 4,
+            "cbig_s_per_iter_at_this_rate": 2.0 * 250000 * 200000 * 4 / (h2d * 1e9),
+            "note": "250000x200000 (200 GB) is larger than this host's 196 GB of RAM; the blockwise path is "
+                    "link-bound and linear in bytes, so its per-iteration time is extrapolated"}
+
+
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -367,9 +416,12 @@ def run_engine_arm(a, rank, world, local_rank):
     if rank == 0 and world == 1 and not a.no_extras:
         extras["plain_arm"] = plain_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm)
         extras["plain_arm"]["fused_speedup"] = value / extras["plain_arm"]["value"]
+        extras["arms"] = {arm: other_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, arm)
+                          for arm in ("bf16x3", "split_bf16", "bf16", "fused_tf32")}
         del V
         torch.cuda.empty_cache()
         extras["sweep"] = sweep_rates(dev)
+        extras["streamed"] = stream_rates(dev)
     if rank != 0:
         return
     line = {"metric": "KL-NMF iterations/s", "value": value, "unit": "iters/s", "n_gpus": world,
@@ -381,6 +433,35 @@ def run_engine_arm(a, rank, world, local_rank):
             "clocks": clk.summary()}
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def other_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, arm, steps=5):
+    """Another fused arm on the same V: iterations/s and its main kernel's HBM fraction."""
+    import torch
+    e = pkg.NMF(n, m, k, arm=arm, device=dev.index or 0)
+    try:
+        e.set_stream(stream.cuda_stream)
+        e.set_V_device(V.data_ptr(), m)
+        e.init_random(3)
+        J = a.iters_per_step
+        for _ in range(3):
+            e.run(J, J, 2 ** 31)
+        e.synchronize()
+        e.profile(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            e.run(J, J, 2 ** 31)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        tot, cnt = e.profile_read(0)
+        e.profile(False)
+    finally:
+        e.close()
+    kms = tot / max(cnt, 1)
+    return {"value": steps * J / (ms / 1e3), "unit": "iters/s", "update_H_kernel_ms": kms,
+            "roofline_frac": n * m * 4 / (kms / 1e3) / 1e9 / hbm}
 
 
 def plain_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, steps=2):

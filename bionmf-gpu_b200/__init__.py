@@ -67,6 +67,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_version": ([], C.c_char_p),
         "nmfb_device_count": ([], i32),
         "nmfb_create": ([C.POINTER(vp), i32, u32, u32, u32, i32], i32),
+        "nmfb_create_streamed": ([C.POINTER(vp), i32, u32, u32, u32, u32], i32),
         "nmfb_destroy": ([vp], i32),
         "nmfb_last_error": ([vp], C.c_char_p),
         "nmfb_set_arm": ([vp, i32], i32),
@@ -153,13 +154,23 @@ class NMF:
     H is exchanged as the reference stores it: m rows of k factors.
     """
 
-    def __init__(self, n: int, m: int, k: int, arm: str | int = "fused", device: int = 0):
+    def __init__(self, n: int, m: int, k: int, arm: str | int = "fused", device: int = 0,
+                 stream_rows: int | None = None):
+        """stream_rows: if given, V stays in host memory and is streamed in
+        blocks of that many rows (0 = automatic) -- the blockwise mode for
+        matrices larger than device memory (plain FP32 arm)."""
         L = load_library()
         self._L = L
         self.n, self.m, self.k = int(n), int(m), int(k)
         self.arm = ARMS[arm] if isinstance(arm, str) else int(arm)
+        self.streamed = stream_rows is not None
+        self._V_keep = None
         h = C.c_void_p()
-        rc = L.nmfb_create(C.byref(h), device, self.n, self.m, self.k, self.arm)
+        if self.streamed:
+            self.arm = ARM_PLAIN
+            rc = L.nmfb_create_streamed(C.byref(h), device, self.n, self.m, self.k, int(stream_rows))
+        else:
+            rc = L.nmfb_create(C.byref(h), device, self.n, self.m, self.k, self.arm)
         self._h = h
         if rc != NMFB_OK:
             msg = L.nmfb_last_error(h).decode() if h else "allocation failed"
@@ -198,6 +209,8 @@ class NMF:
         V = np.ascontiguousarray(V, dtype=np.float32)
         assert V.shape == (self.n, self.m), (V.shape, self.n, self.m)
         self._check(self._L.nmfb_set_V(self._h, _fptr(V), self.m))
+        if self.streamed:
+            self._V_keep = V          # a streamed context reads this host array on every iteration
 
     def set_V_device(self, ptr: int, ld: int):
         self._check(self._L.nmfb_set_V_device(self._h, C.c_void_p(ptr), ld))

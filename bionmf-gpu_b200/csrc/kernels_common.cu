@@ -376,15 +376,22 @@ int nmfb_reset_conv(nmfb_ctx *ctx, uint32_t stop_threshold)
     return NMFB_OK;
 }
 
-int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl)
+int nmfb_objectives_rows(nmfb_ctx *ctx, const float *V, const float *W, uint32_t rows, double out[3])
 {
     unsigned const grid = 4u * (unsigned)ctx->sm_count;
-    k_objective<<<grid, 256, 0, ctx->stream>>>(ctx->dV, ctx->ldv, ctx->dW, ctx->dH, ctx->n, ctx->m, ctx->kp, ctx->k,
-                                              ctx->dObj, ctx->dObj + 3 * 1024, ctx->dObjTicket);
+    k_objective<<<grid, 256, 0, ctx->stream>>>(V, ctx->ldv, W, ctx->dH, rows, ctx->m, ctx->kp, ctx->k, ctx->dObj,
+                                              ctx->dObj + 3 * 1024, ctx->dObjTicket);
     NMFB_LAUNCH_CHECK(ctx);
-    double host[3];
-    NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(host, ctx->dObj + 3 * 1024, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(out, ctx->dObj + 3 * 1024, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return NMFB_OK;
+}
+
+int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl)
+{
+    double host[3];
+    int const rc = ctx->splan ? nmfb_stream_objectives(ctx, host) : nmfb_objectives_rows(ctx, ctx->dV, ctx->dW, ctx->n, host);
+    if (rc) return rc;
     if (dot_V) *dot_V = host[0];
     if (dot_VWH) *dot_VWH = host[1];
     if (kl) *kl = host[2];

@@ -194,5 +194,40 @@ int plain_half(nmfb_ctx *ctx, bool is_H, int adjust)
 
 }  // namespace
 
+// Row-block building blocks for the streamed mode (stream.cu): the same
+// kernels on `rows` rows of W and a rows x ldv block of V / WH.
+int nmfb_plain_wh(nmfb_ctx *ctx, const float *W, uint32_t rows, float *WH)
+{
+    dim3 g((ctx->m + 63) / 64, (rows + 63) / 64);
+    k_gemm_nt<<<g, 256, 0, ctx->stream>>>(W, ctx->dH, WH, rows, ctx->m, ctx->kp, ctx->ldv, ctx->dState);
+    NMFB_LAUNCH_CHECK(ctx);
+    return NMFB_OK;
+}
+
+int nmfb_plain_div(nmfb_ctx *ctx, const float *V, float *WH, uint32_t rows)
+{
+    size_t const total = (size_t)rows * ctx->m;
+    unsigned dg = (unsigned)((total + 255) / 256);
+    if (dg > 16u * (unsigned)ctx->sm_count) dg = 16u * (unsigned)ctx->sm_count;
+    if (dg == 0) dg = 1;
+    k_div<<<dg, 256, 0, ctx->stream>>>(V, WH, rows, ctx->m, ctx->ldv, ctx->dState);
+    NMFB_LAUNCH_CHECK(ctx);
+    return NMFB_OK;
+}
+
+int nmfb_plain_red(nmfb_ctx *ctx, const float *Q, int transQ, const float *F, uint32_t nout, uint32_t nred,
+                   uint32_t *nsplit)
+{
+    RedPlan const p = plan_split(ctx, nout, nred);
+    if ((size_t)p.nsplit * nout * ctx->kp > ctx->part_items)
+        return nmfb_fail(ctx, NMFB_EINVAL, "partial buffer too small (%u splits of %u rows)", p.nsplit, nout);
+    dim3 rg((nout + 63) / 64, p.nsplit);
+    k_gemm_red<<<rg, 256, 0, ctx->stream>>>(Q, ctx->ldv, transQ, F, nout, nred, ctx->kp, p.chunk, ctx->dPart,
+                                           ctx->dState);
+    NMFB_LAUNCH_CHECK(ctx);
+    *nsplit = p.nsplit;
+    return NMFB_OK;
+}
+
 int nmfb_plain_update_H(nmfb_ctx *ctx, int adjust) { return plain_half(ctx, true, adjust); }
 int nmfb_plain_update_W(nmfb_ctx *ctx, int adjust) { return plain_half(ctx, false, adjust); }

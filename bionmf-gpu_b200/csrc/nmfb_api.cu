@@ -50,6 +50,7 @@ void free_all(nmfb_ctx *ctx)
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->hState) cudaFreeHost(ctx->hState);
+    nmfb_stream_release(ctx);
     nmfb_bf16_release(ctx);
     nmfb_fused_release(ctx);
     for (int c = 0; c < 4; c++) {
@@ -95,6 +96,7 @@ int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, 
 
 int do_update_H(nmfb_ctx *ctx, int adjust)
 {
+    if (ctx->splan) return nmfb_stream_update_H(ctx, adjust);
     if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_H(ctx, adjust);
     if (ctx->arm >= NMFB_ARM_BF16) return nmfb_bf16_update_H(ctx, adjust);
     return nmfb_fused_update_H(ctx, adjust);
@@ -102,6 +104,7 @@ int do_update_H(nmfb_ctx *ctx, int adjust)
 
 int do_update_W(nmfb_ctx *ctx, int adjust)
 {
+    if (ctx->splan) return nmfb_stream_update_W(ctx, adjust);
     if (ctx->arm == NMFB_ARM_PLAIN) return nmfb_plain_update_W(ctx, adjust);
     if (ctx->arm >= NMFB_ARM_BF16) return nmfb_bf16_update_W(ctx, adjust);
     return nmfb_fused_update_W(ctx, adjust);
@@ -137,7 +140,8 @@ int nmfb_device_count(void)
     return usable;
 }
 
-int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, int arm)
+static int create_impl(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, int arm, int streamed,
+                       uint32_t block_rows)
 {
     if (!out) return NMFB_EINVAL;
     *out = nullptr;
@@ -177,7 +181,7 @@ int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, 
     size_t const kp = ctx->kp;
     size_t const maxr = n > m ? n : m;
     int rc;
-    if ((rc = dev_alloc(ctx, &ctx->dV, (size_t)n * ctx->ldv, "V"))) return rc;
+    if (!streamed && (rc = dev_alloc(ctx, &ctx->dV, (size_t)n * ctx->ldv, "V"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dW, (size_t)n * kp, "W"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dH, (size_t)m * kp, "H"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dAccW, kp, "accW"))) return rc;
@@ -197,11 +201,26 @@ int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, 
     NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&ctx->hState, 2 * sizeof(ConvState)));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dTickets, 0, 16 * sizeof(uint32_t), ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dObjTicket, 0, 4 * sizeof(uint32_t), ctx->stream));
-    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dV, 0, (size_t)n * ctx->ldv * sizeof(float), ctx->stream));
+    if (ctx->dV) NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dV, 0, (size_t)n * ctx->ldv * sizeof(float), ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dW, 0, (size_t)n * kp * sizeof(float), ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dH, 0, (size_t)m * kp * sizeof(float), ctx->stream));
     if ((rc = nmfb_reset_conv(ctx, 40))) return rc;
+    if (streamed) {
+        if ((rc = nmfb_stream_prepare(ctx, block_rows))) return rc;
+        ctx->arm = NMFB_ARM_PLAIN;
+        return NMFB_OK;
+    }
     return nmfb_set_arm(ctx, arm);
+}
+
+int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, int arm)
+{
+    return create_impl(out, device, n, m, k, arm, 0, 0);
+}
+
+int nmfb_create_streamed(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, uint32_t block_rows)
+{
+    return create_impl(out, device, n, m, k, NMFB_ARM_PLAIN, 1, block_rows);
 }
 
 int nmfb_set_arm(nmfb_ctx *ctx, int arm)
@@ -210,6 +229,11 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
     if (rc) return rc;
     if (arm < NMFB_ARM_FUSED || arm > NMFB_ARM_BF16X3)
         return nmfb_fail(ctx, NMFB_EINVAL, "unknown arm %d", arm);
+    if (ctx->splan) {
+        if (arm != NMFB_ARM_PLAIN)
+            return nmfb_fail(ctx, NMFB_EINVAL, "a streamed-V context runs the plain FP32 arm on row blocks only");
+        return NMFB_OK;
+    }
     if (arm == NMFB_ARM_PLAIN) {
         if (!ctx->dWH && (rc = dev_alloc(ctx, &ctx->dWH, (size_t)ctx->n * ctx->ldv, "WH"))) return rc;
         ctx->arm = arm;
@@ -244,6 +268,11 @@ int nmfb_set_V(nmfb_ctx *ctx, const float *V, size_t ldv)
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!V || ldv < ctx->m) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_V: null V or ldv (%zu) < m (%u)", ldv, ctx->m);
+    if (ctx->splan) {
+        if ((rc = nmfb_stream_set_V(ctx, V, ldv))) return rc;
+        ctx->v_set = 1;
+        return NMFB_OK;
+    }
     NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), V, ldv * sizeof(float),
                                          ctx->m * sizeof(float), ctx->n, cudaMemcpyHostToDevice, ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -256,6 +285,7 @@ int nmfb_set_V_device(nmfb_ctx *ctx, const float *dV, size_t ldv)
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!dV || ldv < ctx->m) return nmfb_fail(ctx, NMFB_EINVAL, "nmfb_set_V_device: null V or ldv < m");
+    if (ctx->splan) return nmfb_fail(ctx, NMFB_ESTATE, "a streamed-V context reads V from host memory (nmfb_set_V)");
     NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), dV, ldv * sizeof(float),
                                          ctx->m * sizeof(float), ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
     ctx->v_set = 1;
@@ -451,6 +481,7 @@ int nmfb_device_factors(nmfb_ctx *ctx, float **dW, float **dH, uint32_t *ldk)
 int nmfb_device_V(nmfb_ctx *ctx, float **dV, size_t *ldv)
 {
     if (!ctx) return NMFB_EINVAL;
+    if (ctx->splan) return nmfb_fail(ctx, NMFB_ESTATE, "a streamed-V context holds no device copy of V");
     if (dV) *dV = ctx->dV;
     if (ldv) *ldv = ctx->ldv;
     return NMFB_OK;

@@ -47,6 +47,7 @@ struct nmfb_ctx {
     int sm_count;
     void *tmaps;           // fused-arm tensor maps (host copy), see kernels_fused.cu
     void *bplan;           // bf16-arm plan, see kernels_bf16.cu
+    void *splan;           // streamed-V plan (V stays in host memory), see stream.cu
 
     // Convergence test state.
     uint32_t *dLabels;     // m
@@ -101,10 +102,23 @@ int nmfb_classify_and_test(nmfb_ctx *ctx, uint32_t niter_test_conv);
 int nmfb_classify_only(nmfb_ctx *ctx);
 int nmfb_reset_conv(nmfb_ctx *ctx, uint32_t stop_threshold);
 int nmfb_objectives(nmfb_ctx *ctx, double *dot_V, double *dot_VWH, double *kl);
+int nmfb_objectives_rows(nmfb_ctx *ctx, const float *V, const float *W, uint32_t rows, double out[3]);
 
 // ---- kernels_plain.cu -----------------------------------------------------
 int nmfb_plain_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_plain_update_W(nmfb_ctx *ctx, int adjust);
+int nmfb_plain_wh(nmfb_ctx *ctx, const float *W, uint32_t rows, float *WH);
+int nmfb_plain_div(nmfb_ctx *ctx, const float *V, float *WH, uint32_t rows);
+int nmfb_plain_red(nmfb_ctx *ctx, const float *Q, int transQ, const float *F, uint32_t nout, uint32_t nred,
+                   uint32_t *nsplit);
+
+// ---- stream.cu --------------------------------------------------------------
+int nmfb_stream_prepare(nmfb_ctx *ctx, uint32_t block_rows);
+int nmfb_stream_release(nmfb_ctx *ctx);
+int nmfb_stream_set_V(nmfb_ctx *ctx, const float *V, size_t ldv);
+int nmfb_stream_update_H(nmfb_ctx *ctx, int adjust);
+int nmfb_stream_update_W(nmfb_ctx *ctx, int adjust);
+int nmfb_stream_objectives(nmfb_ctx *ctx, double out[3]);
 
 // ---- kernels_fused.cu -----------------------------------------------------
 int nmfb_fused_prepare(nmfb_ctx *ctx);

@@ -64,6 +64,18 @@ int nmfb_device_count(void);
  */
 int nmfb_create(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uint32_t k, int arm);
 
+/* Blockwise (out-of-core) mode, for V larger than device memory: the
+ * reference's block plan and partial uploads (src/GPU_setup.c:902-1270,
+ * src/matrix_operations.c:1712-1905).  V is not copied to the device;
+ * nmfb_set_V page-locks the caller's host matrix in place (it must stay valid
+ * and unchanged until the context is destroyed or given another V) and every
+ * half-iteration streams it in blocks of `block_rows` rows (0 = about 256 MB
+ * per block) through two device buffers, the copy of the next block
+ * overlapping the kernels of the current one.  Runs the plain FP32 arm on row
+ * blocks; results equal the resident plain arm's up to FP32 summation order.
+ * nmfb_set_V_device and nmfb_device_V fail with NMFB_ESTATE on such a context. */
+int nmfb_create_streamed(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uint32_t k, uint32_t block_rows);
+
 /* finalize_GPU_device (src/GPU_setup.c:2291): frees everything. NULL is a no-op. */
 int nmfb_destroy(nmfb_ctx *ctx);
 
