@@ -68,6 +68,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_device_count": ([], i32),
         "nmfb_create": ([C.POINTER(vp), i32, u32, u32, u32, i32], i32),
         "nmfb_create_streamed": ([C.POINTER(vp), i32, u32, u32, u32, u32], i32),
+        "nmfb_context_bytes": ([i32, u32, u32, u32, i32, u32], C.c_uint64),
         "nmfb_destroy": ([vp], i32),
         "nmfb_last_error": ([vp], C.c_char_p),
         "nmfb_set_arm": ([vp, i32], i32),
@@ -111,6 +112,12 @@ def load_library(path: str = LIB_PATH):
         f.restype = res
     _lib = L
     return L
+
+
+def context_bytes(n: int, m: int, k: int, arm: str | int = "fused", device: int = 0, stream_rows: int = 0) -> int:
+    """Upper bound of the device memory an NMF(n, m, k, arm) context allocates."""
+    a = ARMS[arm] if isinstance(arm, str) else int(arm)
+    return int(load_library().nmfb_context_bytes(device, n, m, k, a, stream_rows))
 
 
 def device_count() -> int:

@@ -846,13 +846,21 @@ int nmfb_batch_init_random(nmfb_batch *b, const uint32_t *seeds)
         if (e != cudaSuccess) break;
         // CPU_RANDOM initialisation (src/NMF_routines.c:206-233, 299-307):
         // srandom(seed); W (n x k) then H (m x k), random()/RAND_MAX + FLT_MIN.
-        srandom(seeds[p]);
+        // (the generator through a private state: initstate_r / random_r
+        // reproduce srandom / random's sequence without the process-wide one)
+        char rstate[128];
+        struct random_data rd;
+        memset(&rd, 0, sizeof(rd));
+        initstate_r(seeds[p], rstate, sizeof(rstate), &rd);
+        auto next = [&]() -> float {
+            int32_t r;
+            random_r(&rd, &r);
+            return ((float)r) / ((float)RAND_MAX) + FLT_MIN;
+        };
         for (uint32_t i = 0; i < n; i++)
-            for (uint32_t c = 0; c < ks; c++)
-                W[(size_t)i * ks + c] = (c < k) ? ((float)random()) / ((float)RAND_MAX) + FLT_MIN : 0.0f;
+            for (uint32_t c = 0; c < ks; c++) W[(size_t)i * ks + c] = (c < k) ? next() : 0.0f;
         for (uint32_t j = 0; j < m; j++)
-            for (uint32_t c = 0; c < ks; c++)
-                H[(size_t)j * ks + c] = (c < k) ? ((float)random()) / ((float)RAND_MAX) + FLT_MIN : 0.0f;
+            for (uint32_t c = 0; c < ks; c++) H[(size_t)j * ks + c] = (c < k) ? next() : 0.0f;
         e = cudaMemcpyAsync(b->dW + b->woff[p], W, (size_t)n * ks * sizeof(float), cudaMemcpyHostToDevice, b->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(b->dH + b->hoff[p], H, (size_t)m * ks * sizeof(float), cudaMemcpyHostToDevice, b->stream);

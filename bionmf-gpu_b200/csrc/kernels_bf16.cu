@@ -674,8 +674,8 @@ int nmfb_bf16_prepare(nmfb_ctx *ctx)
     // per factor: hi (rows x kp) | lo (rows x kp) | transposed hi and lo blocks (ceil(rows/64) x 2 kp x 64)
     size_t const wsz = (size_t)ctx->n * kp, hsz = (size_t)ctx->m * kp;
     size_t const wt = (size_t)((ctx->n + 63) / 64) * 128 * kp, ht = (size_t)((ctx->m + 63) / 64) * 128 * kp;
-    cudaError_t e = cudaMalloc((void **)&plan->wsplit, (2 * wsz + wt) * sizeof(__nv_bfloat16));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&plan->hsplit, (2 * hsz + ht) * sizeof(__nv_bfloat16));
+    cudaError_t e = nmfb_malloc(ctx, (void **)&plan->wsplit, (2 * wsz + wt) * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->hsplit, (2 * hsz + ht) * sizeof(__nv_bfloat16));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "bf16 split buffers: %s", cudaGetErrorString(e));
     return NMFB_OK;
 }
@@ -684,8 +684,8 @@ int nmfb_bf16_release(nmfb_ctx *ctx)
 {
     PlanB *plan = (PlanB *)ctx->bplan;
     if (!plan) return NMFB_OK;
-    if (plan->wsplit) cudaFree(plan->wsplit);
-    if (plan->hsplit) cudaFree(plan->hsplit);
+    if (plan->wsplit) nmfb_free(ctx, plan->wsplit);
+    if (plan->hsplit) nmfb_free(ctx, plan->hsplit);
     free(plan);
     ctx->bplan = nullptr;
     return NMFB_OK;

@@ -705,12 +705,12 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     FusedPlan *plan = (FusedPlan *)calloc(1, sizeof(FusedPlan));
     if (!plan) return nmfb_fail(ctx, NMFB_ENOMEM, "fused plan");
     ctx->tmaps = plan;
-    cudaError_t e = cudaMalloc((void **)&plan->dErr, sizeof(uint32_t));
+    cudaError_t e = nmfb_malloc(ctx, (void **)&plan->dErr, sizeof(uint32_t));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused error word: %s", cudaGetErrorString(e));
-    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->own_stream));
 #ifdef NMFB_FUSED_DEBUG
-    NMFB_CUDA_TRY(ctx, cudaMalloc((void **)&plan->dDbg, (4 * BO * 64 + 8192) * sizeof(float)));
-    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (4 * BO * 64 + 8192) * sizeof(float), ctx->stream));
+    NMFB_CUDA_TRY(ctx, nmfb_malloc(ctx, (void **)&plan->dDbg, (4 * BO * 64 + 8192) * sizeof(float)));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dDbg, 0, (4 * BO * 64 + 8192) * sizeof(float), ctx->own_stream));
 #endif
     uint32_t const cb = (kp == 16) ? 16 : 32;
     CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
@@ -720,8 +720,8 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     // (ceil(rows / 32) blocks of 2 kp x 32 floats).
     size_t const wsz = (size_t)ctx->n * kp, hsz = (size_t)ctx->m * kp;
     uint32_t const wblk = (ctx->n + 31) / 32, hblk = (ctx->m + 31) / 32;
-    e = cudaMalloc((void **)&plan->dSplitW, (2 * wsz + (size_t)wblk * 64 * kp) * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&plan->dSplitH, (2 * hsz + (size_t)hblk * 64 * kp) * sizeof(float));
+    e = nmfb_malloc(ctx, (void **)&plan->dSplitW, (2 * wsz + (size_t)wblk * 64 * kp) * sizeof(float));
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, (2 * hsz + (size_t)hblk * 64 * kp) * sizeof(float));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused split buffers: %s", cudaGetErrorString(e));
     // update_H: X = H (rows m), Y = W (rows n); V tile [br rows of V][128 cols].
     FusedMaps &mh = plan->mapsH;
@@ -748,9 +748,9 @@ int nmfb_fused_release(nmfb_ctx *ctx)
 {
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
     if (!plan) return NMFB_OK;
-    if (plan->dErr) cudaFree(plan->dErr);
-    if (plan->dSplitW) cudaFree(plan->dSplitW);
-    if (plan->dSplitH) cudaFree(plan->dSplitH);
+    if (plan->dErr) nmfb_free(ctx, plan->dErr);
+    if (plan->dSplitW) nmfb_free(ctx, plan->dSplitW);
+    if (plan->dSplitH) nmfb_free(ctx, plan->dSplitH);
     free(plan);
     ctx->tmaps = nullptr;
     return NMFB_OK;

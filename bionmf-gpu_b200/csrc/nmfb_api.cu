@@ -11,6 +11,16 @@ using nmfb::ConvState;
 
 #define NMFB_VERSION "nmfb200 0.1 (sm_100a)"
 
+cudaError_t nmfb_malloc(nmfb_ctx *ctx, void **p, size_t bytes)
+{
+    return cudaMallocAsync(p, bytes, ctx->own_stream);
+}
+
+void nmfb_free(nmfb_ctx *ctx, void *p)
+{
+    if (p) cudaFreeAsync(p, ctx->own_stream);
+}
+
 namespace {
 
 uint32_t padded_rank(uint32_t k)
@@ -32,7 +42,7 @@ int dev_alloc(nmfb_ctx *ctx, T **p, size_t items, const char *what)
 {
     *p = nullptr;
     if (items == 0) items = 1;
-    cudaError_t e = cudaMalloc((void **)p, items * sizeof(T));
+    cudaError_t e = nmfb_malloc(ctx, (void **)p, items * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -48,7 +58,7 @@ void free_all(nmfb_ctx *ctx)
                     ctx->dPart,    ctx->dColPart, ctx->dTickets, ctx->dObj, ctx->dObjTicket, ctx->dLabels,
                     ctx->dFirst,   ctx->dLastRep, ctx->dState};
     for (void *b : bufs)
-        if (b) cudaFree(b);
+        if (b) nmfb_free(ctx, b);
     if (ctx->hState) cudaFreeHost(ctx->hState);
     nmfb_stream_release(ctx);
     nmfb_bf16_release(ctx);
@@ -208,9 +218,39 @@ static int create_impl(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint3
     if (streamed) {
         if ((rc = nmfb_stream_prepare(ctx, block_rows))) return rc;
         ctx->arm = NMFB_ARM_PLAIN;
-        return NMFB_OK;
+    } else if ((rc = nmfb_set_arm(ctx, arm))) {
+        return rc;
     }
-    return nmfb_set_arm(ctx, arm);
+    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->own_stream));   // allocations usable from any stream
+    return NMFB_OK;
+}
+
+uint64_t nmfb_context_bytes(int device, uint32_t n, uint32_t m, uint32_t k, int arm, uint32_t stream_rows)
+{
+    if (n < 2 || m < 2 || k < 2) return 0;
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    uint64_t const kp = padded_rank(k), ldv = ((uint64_t)m + 31) / 32 * 32, maxr = n > m ? n : m;
+    uint64_t b = 0;
+    uint64_t const nv = (uint64_t)n * ldv * 4;
+    b += stream_rows ? 0 : nv;                                         // V
+    b += ((uint64_t)n + m + 2) * kp * 4;                               // W, H, colsums
+    b += ((uint64_t)512 * sms + 4 * maxr + 256) * kp * 4;               // split partials
+    b += 2 * 1024 * kp * 8 + 64 + (3 * 1024 + 8) * 8 + 16 + (2ull * m + kp) * 4 + 64;   // test / objective state
+    if (stream_rows) {
+        uint64_t const rows = stream_rows < n ? stream_rows : n;
+        b += 3 * rows * ldv * 4 + (uint64_t)m * kp * 4;               // block buffers, Aux
+    } else if (arm == NMFB_ARM_PLAIN) {
+        b += nv;                                                       // WH
+    } else {
+        b += 4 + (2 * ((uint64_t)n + m) + ((n + 31) / 32 + (m + 31) / 32) * 64) * kp * 4;   // TF32 splits
+        if (arm >= NMFB_ARM_BF16)
+            b += (2 * ((uint64_t)n + m) + ((n + 63) / 64 + (m + 63) / 64) * 128) * kp * 2;  // BF16 splits
+    }
+    return b + 32ull * (2u << 20);   // allocation granularity slack for ~32 buffers
 }
 
 int nmfb_create(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint32_t k, int arm)
@@ -236,6 +276,7 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
     }
     if (arm == NMFB_ARM_PLAIN) {
         if (!ctx->dWH && (rc = dev_alloc(ctx, &ctx->dWH, (size_t)ctx->n * ctx->ldv, "WH"))) return rc;
+        if (ctx->stream != ctx->own_stream) NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->own_stream));
         ctx->arm = arm;
         return NMFB_OK;
     }
@@ -243,6 +284,7 @@ int nmfb_set_arm(nmfb_ctx *ctx, int arm)
         return nmfb_fail(ctx, NMFB_EINVAL, "the fused arms support ranks up to 64 (k=%u); use NMFB_ARM_PLAIN", ctx->k);
     if ((rc = nmfb_fused_prepare(ctx))) return rc;
     if (arm >= NMFB_ARM_BF16 && (rc = nmfb_bf16_prepare(ctx))) return rc;
+    if (ctx->stream != ctx->own_stream) NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->own_stream));
     ctx->arm = arm;
     return NMFB_OK;
 }
@@ -305,10 +347,21 @@ int nmfb_init_random(nmfb_ctx *ctx, uint32_t seed)
         return nmfb_fail(ctx, NMFB_ENOMEM, "host allocation for the initial factors");
     }
     // src/NMF_routines.c:206-233 and 299-307: srandom(seed); W first, then H;
-    // (float)random()/(float)RAND_MAX + FLT_MIN per factor entry.
-    srandom(seed);
-    for (size_t e = 0; e < (size_t)n * k; e++) W[e] = ((float)random()) / ((float)RAND_MAX) + FLT_MIN;
-    for (size_t e = 0; e < (size_t)m * k; e++) H[e] = ((float)random()) / ((float)RAND_MAX) + FLT_MIN;
+    // (float)random()/(float)RAND_MAX + FLT_MIN per factor entry.  The same
+    // glibc generator through a private state (initstate_r / random_r with the
+    // default 128-byte state gives srandom/random's sequence), so contexts on
+    // different host threads do not share the process-wide generator.
+    char rstate[128];
+    struct random_data rd;
+    memset(&rd, 0, sizeof(rd));
+    initstate_r(seed, rstate, sizeof(rstate), &rd);
+    auto next = [&]() -> float {
+        int32_t r;
+        random_r(&rd, &r);
+        return ((float)r) / ((float)RAND_MAX) + FLT_MIN;
+    };
+    for (size_t e = 0; e < (size_t)n * k; e++) W[e] = next();
+    for (size_t e = 0; e < (size_t)m * k; e++) H[e] = next();
     rc = nmfb_set_WH(ctx, W, k, H, k);
     free(W);
     free(H);

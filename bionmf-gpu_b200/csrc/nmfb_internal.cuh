@@ -68,6 +68,13 @@ struct nmfb_ctx {
     char err[512];
 };
 
+// ---- device memory -------------------------------------------------------
+// Stream-ordered allocation on the context's own stream (cudaMallocAsync /
+// cudaFreeAsync): creating and destroying contexts while others compute does
+// not synchronise the device, as cudaFree would.
+cudaError_t nmfb_malloc(nmfb_ctx *ctx, void **p, size_t bytes);
+void nmfb_free(nmfb_ctx *ctx, void *p);
+
 // ---- error helpers -------------------------------------------------------
 int nmfb_fail(nmfb_ctx *ctx, int code, const char *fmt, ...);
 

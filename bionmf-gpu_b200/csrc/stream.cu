@@ -102,10 +102,10 @@ int nmfb_stream_prepare(nmfb_ctx *ctx, uint32_t block_rows)
     if (block_rows > ctx->n) block_rows = ctx->n;
     p->rows = block_rows;
     size_t const blk = (size_t)block_rows * ctx->ldv * sizeof(float);
-    cudaError_t e = cudaMalloc((void **)&p->dVb[0], blk);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->dVb[1], blk);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->dWHb, blk);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->dAux, (size_t)ctx->m * ctx->kp * sizeof(float));
+    cudaError_t e = nmfb_malloc(ctx, (void **)&p->dVb[0], blk);
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&p->dVb[1], blk);
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&p->dWHb, blk);
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&p->dAux, (size_t)ctx->m * ctx->kp * sizeof(float));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return nmfb_fail(ctx, NMFB_ENOMEM, "streamed-V block buffers (%u rows): %s", block_rows, cudaGetErrorString(e));
@@ -127,12 +127,12 @@ int nmfb_stream_release(nmfb_ctx *ctx)
     if (p->cs) cudaStreamSynchronize(p->cs);
     if (p->registered) cudaHostUnregister((void *)p->hV);
     for (int s = 0; s < 2; s++) {
-        if (p->dVb[s]) cudaFree(p->dVb[s]);
+        if (p->dVb[s]) nmfb_free(ctx, p->dVb[s]);
         if (p->copied[s]) cudaEventDestroy(p->copied[s]);
         if (p->consumed[s]) cudaEventDestroy(p->consumed[s]);
     }
-    if (p->dWHb) cudaFree(p->dWHb);
-    if (p->dAux) cudaFree(p->dAux);
+    if (p->dWHb) nmfb_free(ctx, p->dWHb);
+    if (p->dAux) nmfb_free(ctx, p->dAux);
     if (p->cs) cudaStreamDestroy(p->cs);
     free(p);
     ctx->splan = nullptr;

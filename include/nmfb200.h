@@ -76,6 +76,13 @@ int nmfb_create(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uint32_t k, 
  * nmfb_set_V_device and nmfb_device_V fail with NMFB_ESTATE on such a context. */
 int nmfb_create_streamed(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uint32_t k, uint32_t block_rows);
 
+/* Device memory a context of these sizes and arm will allocate (bytes, an
+ * upper bound including allocation granularity; stream_rows > 0 for the
+ * blockwise mode), for admission control by a memory budget.  No counterpart
+ * in the reference, which sizes its blocks from the free memory instead
+ * (src/GPU_setup.c:902-1210).  Returns 0 for invalid sizes. */
+uint64_t nmfb_context_bytes(int device, uint32_t n, uint32_t m, uint32_t k, int arm, uint32_t stream_rows);
+
 /* finalize_GPU_device (src/GPU_setup.c:2291): frees everything. NULL is a no-op. */
 int nmfb_destroy(nmfb_ctx *ctx);
 

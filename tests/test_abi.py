@@ -46,3 +46,15 @@ def test_argument_validation_before_device(pkg):
     with pytest.raises(pkg.NMFError) as ei:
         pkg.NMF(1, 5, 2)
     assert ei.value.code == -1
+
+
+def test_context_bytes_accounts_for_each_arm(pkg):
+    n, m, k = 20000, 1000, 16
+    v = n * 1024 * 4
+    fused = pkg.context_bytes(n, m, k, "fused")
+    plain = pkg.context_bytes(n, m, k, "plain")
+    bf16 = pkg.context_bytes(n, m, k, "bf16x3")
+    streamed = pkg.context_bytes(n, m, k, "plain", stream_rows=1000)
+    assert fused > v and plain - fused > v // 2 and bf16 > fused   # plain holds the n x m quotient
+    assert streamed < plain - v               # neither V nor the n x m quotient on the device
+    assert pkg.context_bytes(1, m, k) == 0    # invalid sizes
