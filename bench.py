@@ -301,6 +301,66 @@ def stream_rates(dev, iters=3):
                     "link-bound and linear in bytes, so its per-iteration time is extrapolated"}
 
 
+SERVE = {"requests": 300, "pool": 32, "n": (1000, 50000), "m": (20, 2000), "k": (2, 20), "iters": 300,
+         "budget_gb": 120.0, "workers": 32, "load": 0.8,
+         "desc": "requests n~U[1000,50000], m~logU[20,2000], k~U[2,20], planted Poisson V, 300-iteration cap "
+                 "(-j 10 -t 40: no request can converge before 410 iterations), 120 GB budget"}
+
+
+def serve_requests(dev, count, seed=11):
+    """`count` requests over a pool of planted matrices generated on the device
+    and handed to the server in host memory."""
+    import torch
+    _import_package()
+    import nmf_b200.serve as serve
+    import nmf_b200.synth as synth
+    rng = np.random.default_rng(seed)
+    pool = []
+    for i in range(SERVE["pool"]):
+        n = int(rng.integers(SERVE["n"][0], SERVE["n"][1] + 1))
+        m = int(np.exp(rng.uniform(np.log(SERVE["m"][0]), np.log(SERVE["m"][1]))))
+        kt = int(rng.integers(SERVE["k"][0], SERVE["k"][1] + 1))
+        V, _ = synth.poisson_counts(n, m, min(kt, m), 1000 + i, device=dev)
+        pool.append(V.cpu().numpy())
+        del V
+    torch.cuda.empty_cache()
+    reqs = []
+    for i in range(count):
+        V = pool[int(rng.integers(0, len(pool)))]
+        k = min(int(rng.integers(SERVE["k"][0], SERVE["k"][1] + 1)), V.shape[1])
+        reqs.append(serve.Request(V, k, seed=1 + i, n_iters=SERVE["iters"], niter_test_conv=10, stop_threshold=40,
+                                  rid=i))
+    return reqs
+
+
+def serve_rates(dev, count=None, seq_sample=40):
+    """Serving loop: capacity (all requests queued at once), the sequential
+    baseline (one request at a time, same engine), and an open-loop run with
+    Poisson arrivals at SERVE['load'] of the measured capacity (p50 / p99
+    latency from arrival to result on the host)."""
+    _import_package()
+    import nmf_b200.serve as serve
+    count = count or SERVE["requests"]
+    reqs = serve_requests(dev, count)
+    srv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0)
+    srv.run(reqs[:8], open_loop=False)                       # warm-up (module loads, allocator pools)
+    cap = srv.run(reqs, open_loop=False)
+    seq = srv.run_sequential(reqs[:seq_sample])
+    rate = SERVE["load"] * cap.solves_per_s()
+    arr = serve.poisson_arrivals(count, rate, seed=5)
+    for r, t in zip(reqs, arr):
+        r.arrival = float(t)
+    op = srv.run(reqs, open_loop=True)
+    return {"workload": SERVE["desc"], "requests": count, "value": cap.solves_per_s(), "unit": "solves/s",
+            "sequential": {"value": seq.solves_per_s(), "unit": "solves/s", "sample": f"first {seq_sample} requests"},
+            "speedup_vs_sequential": cap.solves_per_s() / seq.solves_per_s(),
+            "open_loop": {"arrival_rate": rate, "solves_s": op.solves_per_s(), "p50_s": op.latency_pct(50),
+                          "p99_s": op.latency_pct(99), "peak_active": op.peak_active,
+                          "peak_gb": op.peak_bytes / 1e9},
+            "sequential_p50_s_per_request": float(np.median([r.done - r.admitted for r in seq.results])),
+            "workers": SERVE["workers"]}
+
+
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -422,6 +482,7 @@ def run_engine_arm(a, rank, world, local_rank):
         torch.cuda.empty_cache()
         extras["sweep"] = sweep_rates(dev)
         extras["streamed"] = stream_rates(dev)
+        extras["serving"] = serve_rates(dev)
     if rank != 0:
         return
     line = {"metric": "KL-NMF iterations/s", "value": value, "unit": "iters/s", "n_gpus": world,

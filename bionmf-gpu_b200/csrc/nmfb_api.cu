@@ -68,6 +68,7 @@ void free_all(nmfb_ctx *ctx)
         for (int i = 0; i < 2 * NMFB_PROF_POOL; i++) cudaEventDestroy(ctx->prof_ev[c][i]);
         free(ctx->prof_ev[c]);
     }
+    if (ctx->blk_exec) cudaGraphExecDestroy(ctx->blk_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
 }
 
@@ -413,6 +414,56 @@ int nmfb_get_classification(nmfb_ctx *ctx, uint32_t *labels)
     return NMFB_OK;
 }
 
+// One convergence-test block: J iterations (EPS adjust of W in the last
+// update_W) and the classification / connectivity test.
+static int enqueue_block(nmfb_ctx *ctx, uint32_t J)
+{
+    int rc = 0;
+    for (uint32_t i = 0; i < J && rc == 0; i++) {
+        rc = do_update_H(ctx, 0);
+        if (!rc) rc = do_update_W(ctx, i + 1 == J);
+    }
+    if (!rc) rc = nmfb_classify_and_test(ctx, J);
+    return rc;
+}
+
+// Queue one test block, through a CUDA graph captured once per (J, arm,
+// stream) when profiling is off and V is resident; kernel launches otherwise.
+static int launch_block(nmfb_ctx *ctx, uint32_t J)
+{
+    static int const use_graphs = getenv("NMFB_NO_GRAPHS") == nullptr;
+    if (!use_graphs || ctx->prof_on || ctx->splan) return enqueue_block(ctx, J);
+    if (!ctx->blk_exec || ctx->blk_J != J || ctx->blk_arm != ctx->arm || ctx->blk_stream != ctx->stream) {
+        if (ctx->blk_exec) {
+            NMFB_CUDA_TRY(ctx, cudaGraphExecDestroy(ctx->blk_exec));
+            ctx->blk_exec = nullptr;
+        }
+        uint64_t const l0 = ctx->launches;
+        NMFB_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int const rc = enqueue_block(ctx, J);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->blk_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            ctx->blk_exec = nullptr;
+            return nmfb_fail(ctx, NMFB_ECUDA, "capturing the test block: %s", cudaGetErrorString(e));
+        }
+        ctx->blk_kernels = ctx->launches - l0;
+        ctx->launches = l0;
+        ctx->blk_J = J;
+        ctx->blk_arm = ctx->arm;
+        ctx->blk_stream = ctx->stream;
+    }
+    NMFB_CUDA_TRY(ctx, cudaGraphLaunch(ctx->blk_exec, ctx->stream));
+    ctx->launches += ctx->blk_kernels;
+    return NMFB_OK;
+}
+
 int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold, uint32_t *iterations,
              int *converged)
 {
@@ -435,11 +486,7 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     while (b < niter_conv && !stopped) {
         uint32_t const end = (b + batch < niter_conv) ? b + batch : niter_conv;
         for (; b < end; b++) {
-            for (uint32_t i = 0; i < niter_test_conv && rc == 0; i++) {
-                rc = do_update_H(ctx, 0);
-                if (!rc) rc = do_update_W(ctx, i + 1 == niter_test_conv);
-            }
-            if (!rc) rc = nmfb_classify_and_test(ctx, niter_test_conv);
+            rc = launch_block(ctx, niter_test_conv);
             if (rc) break;
         }
         if (rc) break;

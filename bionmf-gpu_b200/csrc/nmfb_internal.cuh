@@ -57,6 +57,14 @@ struct nmfb_ctx {
     nmfb::ConvState *hState;  // pinned host mirror
 
     uint64_t launches;
+    // CUDA graph of one convergence-test block (nmfb_run): replayed instead of
+    // re-launching its ~12 kernels per iteration; rebuilt when J, the arm or
+    // the stream change.
+    cudaGraphExec_t blk_exec;
+    uint32_t blk_J;
+    int blk_arm;
+    cudaStream_t blk_stream;
+    uint64_t blk_kernels;
     cudaStream_t own_stream;
 
     // Event profiling (nmfb_profile): per class a pool of (start, stop) pairs.

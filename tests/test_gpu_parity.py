@@ -156,3 +156,22 @@ def test_engine_matches_reference_fixture(pkg, oracle, case, arm):
         assert maxnorm_rel(e.W, g["W"]) < tol and maxnorm_rel(e.H, g["H"]) < tol
         assert np.array_equal(e.classification(), oracle.classify(g["H"]))
         assert abs(e.distance() - float(g["distance"])) <= 1e-5 * float(g["distance"]) + 5e-7
+
+
+@pytest.mark.parametrize("arm", ["fused", "bf16x3", "plain"])
+def test_graph_replay_matches_kernel_launches(pkg, synth, arm):
+    # nmfb_run replays each test block as a captured CUDA graph unless profiling
+    # is on; both paths must give bit-identical results.
+    V, _ = synth.expression_like(900, 150, 6, seed=17)
+    n, m = V.shape
+    out = []
+    for prof in (False, True):
+        with pkg.NMF(n, m, 6, arm=arm) as e:
+            e.set_V(V)
+            e.init_random(7)
+            e.profile(prof)
+            it = e.run(205, 10, 3)
+            out.append((it, e.W, e.H, e.classification()))
+    (it_g, Wg, Hg, lg), (it_k, Wk, Hk, lk) = out
+    assert it_g == it_k
+    assert np.array_equal(Wg, Wk) and np.array_equal(Hg, Hk) and np.array_equal(lg, lk)
