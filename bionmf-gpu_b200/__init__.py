@@ -69,6 +69,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_create": ([C.POINTER(vp), i32, u32, u32, u32, i32], i32),
         "nmfb_create_streamed": ([C.POINTER(vp), i32, u32, u32, u32, u32], i32),
         "nmfb_context_bytes": ([i32, u32, u32, u32, i32, u32], C.c_uint64),
+        "nmfb_release_cached": ([i32], i32),
         "nmfb_destroy": ([vp], i32),
         "nmfb_last_error": ([vp], C.c_char_p),
         "nmfb_set_arm": ([vp, i32], i32),

@@ -34,7 +34,10 @@ __device__ __forceinline__ float adjust_value(float v) { return fmaxf(v, FLT_MIN
 
 // ---------------------------------------------------------------------------
 // Column sums: block b reduces rows [r0, r1) of X (rows x kp) into part[b][*];
-// the last block to retire sums the block partials in block order (FP64).
+// the last block to retire sums the block partials (FP64) in a fixed order:
+// thread group g (of blockDim / kp) sums blocks g, g + groups, ... in order,
+// then the groups are added in order.  Many short blocks with four loads in
+// flight per thread keep the reads bandwidth-bound rather than latency-bound.
 __global__ void k_colsum(const float *__restrict__ X, uint32_t rows, uint32_t kp, double *__restrict__ part,
                          float *__restrict__ acc, uint32_t *__restrict__ ticket, const ConvState *st)
 {
@@ -48,9 +51,18 @@ __global__ void k_colsum(const float *__restrict__ X, uint32_t rows, uint32_t kp
     uint32_t const r0 = blockIdx.x * per;
     uint32_t const r1 = min(rows, r0 + per);
     double s = 0.0;
-    if (rl < lanes)
-        for (uint32_t r = r0 + rl; r < r1; r += lanes)
-            s += (double)X[(size_t)r * kp + c];
+    if (rl < lanes) {
+        uint32_t r = r0 + rl;
+        for (; r + 3 * lanes < r1; r += 4 * lanes) {
+            float const a0 = X[(size_t)r * kp + c], a1 = X[(size_t)(r + lanes) * kp + c];
+            float const a2 = X[(size_t)(r + 2 * lanes) * kp + c], a3 = X[(size_t)(r + 3 * lanes) * kp + c];
+            s += (double)a0;
+            s += (double)a1;
+            s += (double)a2;
+            s += (double)a3;
+        }
+        for (; r < r1; r += lanes) s += (double)X[(size_t)r * kp + c];
+    }
     red[threadIdx.x] = s;
     __syncthreads();
     if (threadIdx.x < kp) {
@@ -66,11 +78,16 @@ __global__ void k_colsum(const float *__restrict__ X, uint32_t rows, uint32_t kp
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    for (uint32_t cc = threadIdx.x; cc < kp; cc += blockDim.x) {
-        double t = 0.0;
-        for (uint32_t b = 0; b < gridDim.x; b++)
-            t += __ldcg(&part[(size_t)b * kp + cc]);
-        acc[cc] = (float)t;
+    uint32_t const groups = lanes;
+    double t = 0.0;
+    if (rl < groups)
+        for (uint32_t b = rl; b < gridDim.x; b += groups) t += __ldcg(&part[(size_t)b * kp + c]);
+    red[threadIdx.x] = t;
+    __syncthreads();
+    if (threadIdx.x < kp) {
+        double u = 0.0;
+        for (uint32_t g = 0; g < groups; g++) u += red[g * kp + threadIdx.x];
+        acc[threadIdx.x] = (float)u;
     }
     if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -287,8 +304,8 @@ inline unsigned grid_for(size_t items, unsigned block, unsigned cap)
 int nmfb_colsum(nmfb_ctx *ctx, const float *X, uint32_t rows, float *acc, int which)
 {
     unsigned const block = 256;
-    unsigned grid = (rows + 255) / 256;
-    if (grid > 2u * (unsigned)ctx->sm_count) grid = 2u * (unsigned)ctx->sm_count;
+    unsigned grid = (rows + 31) / 32;        // ~32 rows per block; at most 1024 block partials
+    if (grid > 1024u) grid = 1024u;
     if (grid < 1) grid = 1;
     k_colsum<<<grid, block, 0, ctx->stream>>>(X, rows, ctx->kp, ctx->dColPart + (size_t)which * 1024 * ctx->kp, acc,
                                              ctx->dTickets + which, ctx->dState);

@@ -5,15 +5,68 @@
 #include <float.h>
 #include <math.h>
 #include <stdlib.h>
+#include <mutex>
 #include <new>
 
 using nmfb::ConvState;
 
 #define NMFB_VERSION "nmfb200 0.1 (sm_100a)"
 
+// One library-owned stream-ordered memory pool per device; freed blocks stay
+// in the pool for the next context (no device-wide synchronisation and no new
+// mappings when contexts come and go) until nmfb_release_cached trims it.
+static std::mutex g_pool_mutex;
+static cudaMemPool_t g_pools[64];
+
+static cudaError_t device_pool(int device, cudaMemPool_t *out)
+{
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+        g_pools[device] = pool;
+    }
+    *out = g_pools[device];
+    return cudaSuccess;
+}
+
 cudaError_t nmfb_malloc(nmfb_ctx *ctx, void **p, size_t bytes)
 {
-    return cudaMallocAsync(p, bytes, ctx->own_stream);
+    cudaMemPool_t pool;
+    cudaError_t e = device_pool(ctx->device, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, bytes, pool, ctx->own_stream);
+}
+
+int nmfb_release_cached(int device)
+{
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (device >= 0 && device < 64) pool = g_pools[device];
+    }
+    if (!pool) return NMFB_OK;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return NMFB_ECUDA;
+    if (cudaSetDevice(device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaSetDevice(prev);
+        return NMFB_ECUDA;
+    }
+    cudaSetDevice(prev);
+    return NMFB_OK;
 }
 
 void nmfb_free(nmfb_ctx *ctx, void *p)
@@ -175,13 +228,15 @@ static int create_impl(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint3
         cudaGetLastError();
         return nmfb_fail(ctx, NMFB_ENODEV, "no CUDA device %d (devices: %d)", device, ndev);
     }
-    cudaDeviceProp prop;
-    NMFB_CUDA_TRY(ctx, cudaGetDeviceProperties(&prop, device));
-    if (prop.major != 10)
+    int major = 0, minor = 0, sms = 0;
+    NMFB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    NMFB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+    NMFB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    if (major != 10)
         return nmfb_fail(ctx, NMFB_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a only", device,
-                         prop.major, prop.minor);
+                         major, minor);
     NMFB_CUDA_TRY(ctx, cudaSetDevice(device));
-    ctx->sm_count = prop.multiProcessorCount;
+    ctx->sm_count = sms;
     NMFB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
     ctx->stream = ctx->own_stream;
     ctx->n = n;

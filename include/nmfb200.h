@@ -83,6 +83,13 @@ int nmfb_create_streamed(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uin
  * (src/GPU_setup.c:902-1210).  Returns 0 for invalid sizes. */
 uint64_t nmfb_context_bytes(int device, uint32_t n, uint32_t m, uint32_t k, int arm, uint32_t stream_rows);
 
+/* Context device memory comes from a library-owned stream-ordered pool per
+ * device (cudaMallocFromPoolAsync), so contexts can be created and destroyed
+ * while others compute without synchronising the device.  Freed memory stays
+ * cached in the pool for the next context; this returns it to the driver
+ * (after synchronising the device).  No counterpart in the reference. */
+int nmfb_release_cached(int device);
+
 /* finalize_GPU_device (src/GPU_setup.c:2291): frees everything. NULL is a no-op. */
 int nmfb_destroy(nmfb_ctx *ctx);
 
