@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
-        // Two issue queues, polled without blocking (nanosleep back-off):
+        // Two issue queues, polled without blocking (shortest nanosleep between polls):
         //   MMA2(n2): needs the R warps' R(n2) and, for n2 >= 2, the accumulator
         //             warps to have read Acc[n2 % 2] of tile n2-2;
         //   MMA1(n1): needs Y(n1) loaded and a free D buffer (MMA2(n1-NDB)
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                     atomicExch(args.err, 4u);
                     ok = false;
                 } else {
-                    __nanosleep(64);
+                    __nanosleep(0);
                 }
             }
         }
@@ -506,12 +506,14 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
 #pragma unroll
             for (int part = 0; part < (NTERMS == 3 ? 2 : 1); part++) {
 #pragma unroll
-                for (int c0 = 0; c0 < KP; c0 += 16) {
+                for (int c0 = 0; c0 < KP; c0 += 32) {
                     uint32_t a[32];
-                    tmem_ld16(lane_addr + bp * ACC_COLS + part * KP + c0, a);
+                    if (KP - c0 >= 32) tmem_ld32(lane_addr + bp * ACC_COLS + part * KP + c0, a);
+                    else tmem_ld16(lane_addr + bp * ACC_COLS + part * KP + c0, a);
                     tmem_wait_ld_dep(a);
 #pragma unroll
-                    for (int c = 0; c < 16; c++) sum[c0 + c] += __uint_as_float(a[c]);
+                    for (int c = 0; c < 32; c++)
+                        if (c0 + c < KP) sum[c0 + c] += __uint_as_float(a[c]);
                 }
             }
             tc_fence_before();
