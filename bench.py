@@ -214,7 +214,7 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
     seeds = np.tile(np.arange(1, R + 1, dtype=np.uint32), len(ks))
     nprob = len(ranks)
     flush = flush or L2Flush(dev)
-    dev_ms, e2e_ms, iters = [], [], None
+    dev_ms, e2e_ms, iters, ctas = [], [], None, 1
     with pkg.Batch(n, m, ranks, device=dev.index or 0) as b:
         for s in range(warmup + steps):
             torch.cuda.synchronize()
@@ -224,6 +224,7 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
             b.set_V(V)
             b.init_random(seeds)
             it, conv = b.run(2000, 10, 40)
+            ctas = b.cluster
             b.classification()
             coph = {k: b.consensus(k)[2] for k in ks}
             t1 = time.perf_counter()
@@ -252,7 +253,7 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
             "sequential": {"value": seq, "unit": "solves/s", "sample": f"{seq_n} solves (k=2..10 x {seq_sample} seeds), "
                                                                       "single-problem engine, host-timed"},
             "speedup_vs_sequential": batched / seq, "tflops": flops / (statistics.median(dev_ms) / 1e3) / 1e12,
-            "mean_iterations": float(np.mean(iters)), "cophenetic": {str(k): round(v, 6) for k, v in coph.items()},
+            "mean_iterations": float(np.mean(iters)), "ctas_per_problem": ctas, "cophenetic": {str(k): round(v, 6) for k, v in coph.items()},
             "l2": "256 MB buffer written before every sweep"}
 
 

@@ -101,6 +101,8 @@ def load_library(path: str = LIB_PATH):
         "nmfb_batch_init_random": ([vp, C.POINTER(u32)], i32),
         "nmfb_batch_set_WH": ([vp, u32, fp, sz, fp, sz], i32),
         "nmfb_batch_set_tiles": ([vp, u32, u32, u32], i32),
+        "nmfb_batch_set_cluster": ([vp, u32], i32),
+        "nmfb_batch_get_cluster": ([vp, C.POINTER(u32)], i32),
         "nmfb_batch_run": ([vp, u32, u32, u32, C.POINTER(u32), C.POINTER(i32)], i32),
         "nmfb_batch_last_ms": ([vp, C.POINTER(C.c_double)], i32),
         "nmfb_batch_get_classification": ([vp, C.POINTER(u32)], i32),
@@ -373,6 +375,17 @@ class Batch:
 
     def set_tiles(self, p: int, wt: int, jt: int):
         self._check(self._L.nmfb_batch_set_tiles(self._h, p, wt, jt))
+
+    def set_cluster(self, ctas: int):
+        """CTAs per problem (1, 2, 4, 8; 0 = automatic); see nmfb_batch_set_cluster."""
+        self._check(self._L.nmfb_batch_set_cluster(self._h, ctas))
+
+    @property
+    def cluster(self) -> int:
+        """CTAs per problem of the last run."""
+        c = C.c_uint32()
+        self._check(self._L.nmfb_batch_get_cluster(self._h, C.byref(c)))
+        return int(c.value)
 
     def run(self, n_iters=2000, niter_test_conv=10, stop_threshold=40):
         """Returns (iterations, converged) arrays, one entry per problem."""

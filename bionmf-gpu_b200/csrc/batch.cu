@@ -10,10 +10,18 @@
 // (src/common.c:1195-1209) with the stop rule of src/NMF_GPU.c:695-709; the
 // remaining n_iters % niter_test_conv iterations run without adjust.
 //
-// Work distribution: persistent CTAs (occupancy x SMs, at most one per
-// problem) take problems from an atomic work queue in the order the host gives
-// (largest rank first), and one CTA runs one problem to its end.  Problems are
-// independent, so no CTA ever waits on another.
+// Work distribution: persistent thread-block clusters of C CTAs (C = 1, 2, 4
+// or 8; as many clusters as fit on the GPU, at most one per problem) take
+// problems from an atomic work queue in the order the host gives (largest rank
+// first), and one cluster runs one problem to its end.  Within a cluster, CTA r
+// owns a contiguous slice of W's rows and every CTA holds the whole of H: the
+// update_H partial sums over W's rows and the partial column sums of W are
+// added across the cluster in rank order through distributed shared memory, so
+// every CTA computes the same H, the same classification and the same stop
+// decision.  Convergence iteration counts are data dependent (a sweep's
+// problems stop after 430 to 2000 iterations), so with one CTA per problem the
+// few longest problems set the launch time; splitting each problem over C SMs
+// divides that tail by about C.  C = 1 keeps the single-CTA summation order.
 //
 // Per problem, in one CTA of NT = 256 threads:
 //   shared memory: H (m x ks, ks = k rounded up to 4), a staging tile (rows of
@@ -43,6 +51,10 @@
 #include <algorithm>
 #include <new>
 #include <vector>
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -78,7 +90,7 @@ __host__ __device__ constexpr uint32_t ks_of(uint32_t k) { return (k + 3u) & ~3u
 //             (16-byte aligned rows; float4 reads of 8 consecutive rows hit
 //             8 distinct bank groups).
 struct SmemLayout {
-    uint32_t h, stage, red, accw, acch, lab, rep, first, total;
+    uint32_t h, stage, red, accw, acch, lab, rep, first, part, partw, total;
     uint32_t cs, hbuf, wbuf, vst;   // update_H column span and buffer sizes; update_W row stride
 };
 __host__ __device__ inline SmemLayout smem_layout(uint32_t m, uint32_t ks, uint32_t wt, uint32_t jt, uint64_t ldv)
@@ -97,7 +109,9 @@ __host__ __device__ inline SmemLayout smem_layout(uint32_t m, uint32_t ks, uint3
     L.lab = L.acch + ks;
     L.rep = L.lab + m;
     L.first = L.rep + m;
-    L.total = L.first + 32;
+    L.part = L.first + 32;                 // this CTA's update_H partials (m x ks), read by the cluster
+    L.partw = L.part + ((m * ks + 3u) & ~3u);   // this CTA's partial column sums of W (ks)
+    L.total = L.partw + ks;
     return L;
 }
 
@@ -166,6 +180,38 @@ __device__ __forceinline__ void block_sum(float (&v)[K], float *red, float *out,
     __syncthreads();
 }
 
+// This CTA's place in its problem's cluster: rank, cluster size and the rows
+// [r0, r1) of W it owns.
+struct Slice {
+    uint32_t rank, size, r0, r1;
+};
+
+// Sum over the cluster, in rank order, of the float at offset `off` of every
+// CTA's shared memory (this CTA's own included).
+__device__ __forceinline__ float cluster_sum(float *sm, uint32_t off, uint32_t csize)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    float s = 0.0f;
+    for (uint32_t q = 0; q < csize; q++) s += cl.map_shared_rank(sm, q)[off];
+    return s;
+}
+
+// colsum(W) into accw: this CTA's rows (wsum, per thread), then for a cluster
+// the partials of every CTA added in rank order.
+template <int K>
+__device__ void colsum_W(float (&wsum)[K], float *sm, const SmemLayout &L, const Slice &X)
+{
+    constexpr uint32_t KS = ks_of(K);
+    if (X.size == 1) {
+        block_sum<K>(wsum, sm + L.red, sm + L.accw, KS);
+        return;
+    }
+    block_sum<K>(wsum, sm + L.red, sm + L.partw, KS);
+    cg::this_cluster().sync();   // every CTA's partial column sums are written
+    if (threadIdx.x < (uint32_t)K) sm[L.accw + threadIdx.x] = cluster_sum(sm, L.partw + threadIdx.x, X.size);
+    __syncthreads();
+}
+
 // update_H: stage tile t (rows of V for columns [j0, j0+cs) and rows of W) into buffer b.
 template <uint32_t KS>
 __device__ __forceinline__ void stage_H(const Problem &P, float *buf, const SmemLayout &L, uint32_t j0, uint32_t i0,
@@ -190,16 +236,21 @@ __device__ __forceinline__ void stage_H(const Problem &P, float *buf, const Smem
     for (uint32_t e = threadIdx.x; e < rows * (KS / 4); e += NT) cp_async16(sW + 4 * e, src + 4 * e);
 }
 
+// With a cluster, each CTA sums over its own rows of W into `part`; after a
+// cluster barrier every CTA adds the partials of all CTAs in rank order and
+// updates its copy of H (the same values in every CTA).  The next write of
+// `part` comes after the cluster barrier of the following colsum_W, so no CTA
+// overwrites partials that another may still read.
 template <int K>
-__device__ void update_H(const Problem &P, float *sm, const SmemLayout &L)
+__device__ void update_H(const Problem &P, float *sm, const SmemLayout &L, const Slice &X)
 {
     constexpr uint32_t KS = ks_of(K);
     float *sH = sm + L.h;
     float *stage = sm + L.stage;
     uint32_t const half = (L.hbuf > L.wbuf ? L.hbuf : L.wbuf);
     const float *accW = sm + L.accw;
-    uint32_t const tid = threadIdx.x, n = P.n, m = P.m, wt = P.wt;
-    uint32_t const ntiles = (n + wt - 1) / wt;
+    uint32_t const tid = threadIdx.x, m = P.m, wt = P.wt;
+    uint32_t const ntiles = (X.r1 - X.r0 + wt - 1) / wt;
     float hsum[K];
 #pragma unroll
     for (int c = 0; c < K; c++) hsum[c] = 0.0f;
@@ -213,12 +264,12 @@ __device__ void update_H(const Problem &P, float *sm, const SmemLayout &L)
             acc[c] = 0.0f;
         }
         __syncthreads();   // the staging region may still be read by the previous phase
-        stage_H<KS>(P, stage, L, j0, 0, min(wt, n));
+        if (ntiles) stage_H<KS>(P, stage, L, j0, X.r0, min(wt, X.r1 - X.r0));
         cp_async_commit();
         for (uint32_t t = 0; t < ntiles; t++) {
-            uint32_t const i0 = t * wt;
-            uint32_t const rows = min(wt, n - i0);
-            if (t + 1 < ntiles) stage_H<KS>(P, stage + ((t + 1) & 1) * half, L, j0, i0 + wt, min(wt, n - i0 - wt));
+            uint32_t const i0 = X.r0 + t * wt;
+            uint32_t const rows = min(wt, X.r1 - i0);
+            if (t + 1 < ntiles) stage_H<KS>(P, stage + ((t + 1) & 1) * half, L, j0, i0 + wt, min(wt, X.r1 - i0 - wt));
             cp_async_commit();
             cp_async_wait1();
             __syncthreads();
@@ -240,13 +291,29 @@ __device__ void update_H(const Problem &P, float *sm, const SmemLayout &L)
             __syncthreads();
         }
         if (active) {
+            if (X.size == 1) {
+#pragma unroll
+                for (int c = 0; c < K; c++) {
+                    float const hn = __fdiv_rn(h[c] * acc[c], accW[c]);
+                    sH[j * KS + c] = hn;
+                    hsum[c] += hn;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < K; c++) sm[L.part + j * KS + c] = acc[c];
+            }
+        }
+    }
+    if (X.size > 1) {
+        cg::this_cluster().sync();   // every CTA's partials are written
+        for (uint32_t j = tid; j < m; j += NT)
 #pragma unroll
             for (int c = 0; c < K; c++) {
-                float const hn = __fdiv_rn(h[c] * acc[c], accW[c]);
+                float const tot = cluster_sum(sm, L.part + j * KS + c, X.size);
+                float const hn = __fdiv_rn(sH[j * KS + c] * tot, accW[c]);
                 sH[j * KS + c] = hn;
                 hsum[c] += hn;
             }
-        }
     }
     block_sum<K>(hsum, sm + L.red, sm + L.acch, KS);
 }
@@ -265,22 +332,22 @@ __device__ __forceinline__ void stage_W(const Problem &P, float *buf, const Smem
 }
 
 template <int K>
-__device__ void update_W(const Problem &P, float *sm, const SmemLayout &L, bool adjust)
+__device__ void update_W(const Problem &P, float *sm, const SmemLayout &L, bool adjust, const Slice &X)
 {
     constexpr uint32_t KS = ks_of(K);
     const float *sH = sm + L.h;
     float *stage = sm + L.stage;
     uint32_t const half = (L.hbuf > L.wbuf ? L.hbuf : L.wbuf);
     const float *accH = sm + L.acch;
-    uint32_t const tid = threadIdx.x, n = P.n, m = P.m, jt = P.jt;
+    uint32_t const tid = threadIdx.x, m = P.m, jt = P.jt;
     uint32_t const ntiles = (m + jt - 1) / jt;
     float wsum[K];
 #pragma unroll
     for (int c = 0; c < K; c++) wsum[c] = 0.0f;
-    for (uint32_t i0 = 0; i0 < n; i0 += NT) {
+    for (uint32_t i0 = X.r0; i0 < X.r1; i0 += NT) {
         uint32_t const i = i0 + tid;
-        bool const active = i < n;
-        uint32_t const rows = min((uint32_t)NT, n - i0);
+        bool const active = i < X.r1;
+        uint32_t const rows = min((uint32_t)NT, X.r1 - i0);
         float w[K], aux[K];
 #pragma unroll
         for (int c = 0; c < K; c++) {
@@ -336,7 +403,7 @@ __device__ void update_W(const Problem &P, float *sm, const SmemLayout &L, bool 
             }
         }
     }
-    block_sum<K>(wsum, sm + L.red, sm + L.accw, KS);
+    colsum_W<K>(wsum, sm, L, X);
 }
 
 // Warp-per-sample classification of H with the reference's tie rule (k <= 32:
@@ -381,11 +448,11 @@ __device__ void classify(float *sm, const SmemLayout &L, uint32_t m, bool adjust
 }
 
 template <int K>
-__device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *s_ctl)
+__device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *s_ctl, const Slice &X)
 {
     constexpr uint32_t KS = ks_of(K);
     SmemLayout const L = smem_layout(P.m, KS, P.wt, P.jt, P.ldv);
-    uint32_t const tid = threadIdx.x, m = P.m, n = P.n;
+    uint32_t const tid = threadIdx.x, m = P.m;
     uint32_t *lab = reinterpret_cast<uint32_t *>(sm + L.lab);
     uint32_t *rep = reinterpret_cast<uint32_t *>(sm + L.rep);
     uint32_t *first = reinterpret_cast<uint32_t *>(sm + L.first);
@@ -407,19 +474,19 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
         float ws[K];
 #pragma unroll
         for (int c = 0; c < K; c++) ws[c] = 0.0f;
-        for (uint32_t i = tid; i < n; i += NT)
+        for (uint32_t i = X.r0 + tid; i < X.r1; i += NT)
 #pragma unroll
             for (int c = 0; c < K; c++) ws[c] += P.W[(size_t)i * KS + c];
         __syncthreads();
-        block_sum<K>(ws, sm + L.red, sm + L.accw, KS);
+        colsum_W<K>(ws, sm, L, X);
     }
 
     uint32_t const J = A.niter_test_conv;
     uint32_t const nblocks = A.n_iters / J, rem = A.n_iters % J;
     for (uint32_t b = 0; b < nblocks; b++) {
         for (uint32_t it = 0; it < J; it++) {
-            update_H<K>(P, sm, L);
-            update_W<K>(P, sm, L, it + 1 == J);
+            update_H<K>(P, sm, L, X);
+            update_W<K>(P, sm, L, it + 1 == J, X);
         }
         classify<K>(sm, L, m, true);
         uint32_t local = 0;
@@ -444,13 +511,14 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
     }
     if (!s_ctl[1])
         for (uint32_t it = 0; it < rem; it++) {
-            update_H<K>(P, sm, L);
-            update_W<K>(P, sm, L, false);
+            update_H<K>(P, sm, L, X);
+            update_W<K>(P, sm, L, false, X);
         }
-    // final classification (no adjust) and write-back
+    // final classification (no adjust) and write-back (every CTA of a cluster
+    // holds the same H and labels; rank 0 writes them)
     classify<K>(sm, L, m, false);
-    for (uint32_t j = tid; j < m; j += NT) P.labels[j] = lab[j];
-    {
+    if (X.rank == 0) {
+        for (uint32_t j = tid; j < m; j += NT) P.labels[j] = lab[j];
         const float4 *src = reinterpret_cast<const float4 *>(sm + L.h);
         float4 *dst = reinterpret_cast<float4 *>(P.H);
         for (uint32_t e = tid; e < m * KS / 4; e += NT) dst[e] = src[e];
@@ -470,16 +538,29 @@ __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, co
     float *sm = reinterpret_cast<float *>(smem4);
     __shared__ uint32_t s_next;
     __shared__ uint32_t s_ctl[4];
+    cg::cluster_group const cl = cg::this_cluster();
+    uint32_t const crank = cl.block_rank(), csize = cl.num_blocks();
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
-        __syncthreads();
-        uint32_t const q = s_next;
+        if (crank == 0 && threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
+        uint32_t q;
+        if (csize > 1) {
+            cl.sync();
+            q = *cl.map_shared_rank(&s_next, 0u);
+            // rank 0 rewrites s_next, and any CTA may leave the kernel, only after
+            // every CTA has read it (and, earlier, every partial it needed)
+            cl.sync();
+        } else {
+            __syncthreads();
+            q = s_next;
+        }
         if (q >= nprob) break;
         Problem P = probs[order[q]];
+        uint32_t const chunk = (P.n + csize - 1) / csize;
+        Slice const X{crank, csize, min(P.n, crank * chunk), min(P.n, crank * chunk + chunk)};
         switch (P.k) {
 #define NMFB_BATCH_CASE(KK) \
-    case KK: run_problem<KK>(P, sm, A, s_ctl); break;
+    case KK: run_problem<KK>(P, sm, A, s_ctl, X); break;
             NMFB_BATCH_CASE(2) NMFB_BATCH_CASE(3) NMFB_BATCH_CASE(4) NMFB_BATCH_CASE(5) NMFB_BATCH_CASE(6)
             NMFB_BATCH_CASE(7) NMFB_BATCH_CASE(8) NMFB_BATCH_CASE(9) NMFB_BATCH_CASE(10) NMFB_BATCH_CASE(11)
             NMFB_BATCH_CASE(12) NMFB_BATCH_CASE(13) NMFB_BATCH_CASE(14) NMFB_BATCH_CASE(15) NMFB_BATCH_CASE(16)
@@ -487,7 +568,7 @@ __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, co
 #undef NMFB_BATCH_CASE
             default: break;
         }
-        if (threadIdx.x == 0) {
+        if (crank == 0 && threadIdx.x == 0) {
             Problem *dst = probs + order[q];
             dst->iterations = P.iterations;
             dst->converged = P.converged;
@@ -664,6 +745,8 @@ struct nmfb_batch {
     size_t smem_optin;
     std::vector<uint32_t> ranks;
     std::vector<uint32_t> wt, jt;        // per-problem tile shapes
+    uint32_t cluster;                     // CTAs per problem (0 = automatic)
+    uint32_t last_cluster;                // the value the last run used
     float *dV;
     float *dW, *dH;                       // per-problem slices (n x ks, m x ks)
     std::vector<size_t> woff, hoff;       // float offsets of each problem's slices
@@ -899,6 +982,22 @@ int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt)
     return NMFB_OK;
 }
 
+int nmfb_batch_set_cluster(nmfb_batch *b, uint32_t ctas)
+{
+    if (!b) return NMFB_EINVAL;
+    if (ctas != 0 && ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8)
+        return bfail(b, NMFB_EINVAL, "CTAs per problem must be 0 (automatic), 1, 2, 4 or 8");
+    b->cluster = ctas;
+    return NMFB_OK;
+}
+
+int nmfb_batch_get_cluster(const nmfb_batch *b, uint32_t *ctas)
+{
+    if (!b || !ctas) return NMFB_EINVAL;
+    *ctas = b->last_cluster;
+    return NMFB_OK;
+}
+
 int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold,
                    uint32_t *iterations, int *converged)
 {
@@ -924,12 +1023,33 @@ int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, ui
     int per_sm = 0;
     BTRY(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, NT, smem));
     if (per_sm < 1) return bfail(b, NMFB_EINVAL, "batched kernel does not fit on an SM with %zu B shared memory", smem);
-    uint32_t grid = (uint32_t)per_sm * (uint32_t)b->sm_count;
-    if (grid > b->nprob) grid = b->nprob;
+    // CTAs per problem: automatic = 8 when the batch leaves most CTA slots idle
+    // at one problem per 8 CTAs, else 4 (a problem's time shrinks about C-fold,
+    // so the few problems that run to the iteration cap no longer set the
+    // launch time).
+    uint32_t const slots = (uint32_t)per_sm * (uint32_t)b->sm_count;
+    uint32_t C = b->cluster ? b->cluster : ((uint64_t)b->nprob * 8 <= slots ? 8u : 4u);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * (uint32_t)b->sm_count, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = b->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    BTRY(b, cudaOccupancyMaxActiveClusters(&nclusters, k_batch, &cfg));
+    if (nclusters < 1) return bfail(b, NMFB_EINVAL, "no cluster of %u batched CTAs fits on the device", C);
+    uint32_t ncl = (uint32_t)nclusters < b->nprob ? (uint32_t)nclusters : b->nprob;
+    cfg.gridDim = dim3(ncl * C, 1, 1);
+    b->last_cluster = C;
     LoopArgs A{n_iters, niter_test_conv, stop_threshold};
     BTRY(b, cudaEventRecord(b->ev0, b->stream));
-    k_batch<<<grid, NT, smem, b->stream>>>(b->dProbs, b->dOrder, b->nprob, b->dQueue, A);
-    BTRY(b, cudaGetLastError());
+    BTRY(b, cudaLaunchKernelEx(&cfg, k_batch, b->dProbs, (const uint32_t *)b->dOrder, b->nprob, b->dQueue, A));
     BTRY(b, cudaEventRecord(b->ev1, b->stream));
     BTRY(b, cudaMemcpyAsync(P.data(), b->dProbs, b->nprob * sizeof(Problem), cudaMemcpyDeviceToHost, b->stream));
     BTRY(b, cudaStreamSynchronize(b->stream));

@@ -218,6 +218,16 @@ int nmfb_batch_set_WH(nmfb_batch *b, uint32_t p, const float *W, size_t ldw, con
  * 8..512), jt columns of V per update_W tile (a power of two, 4..64). */
 int nmfb_batch_set_tiles(nmfb_batch *b, uint32_t p, uint32_t wt, uint32_t jt);
 
+/* CTAs that share each problem (a thread-block cluster; no counterpart in the
+ * reference, which runs one problem per process): 1, 2, 4 or 8, or 0 for the
+ * automatic choice (8 when nprob * 8 fits the CTA slots of the device, else 4).
+ * The CTAs split W's rows and add their partial sums in a fixed order, so a
+ * result depends on this value but is the same on every run with it; 1 keeps
+ * the single-CTA summation order.  nmfb_batch_get_cluster reports the value
+ * the last nmfb_batch_run used. */
+int nmfb_batch_set_cluster(nmfb_batch *b, uint32_t ctas);
+int nmfb_batch_get_cluster(const nmfb_batch *b, uint32_t *ctas);
+
 /* Run every problem to convergence or n_iters with the reference's rules
  * (-i n_iters, -j niter_test_conv, -t stop_threshold).  iterations[p] and
  * converged[p] (either may be NULL) as nmfb_run reports them. */

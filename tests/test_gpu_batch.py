@@ -5,7 +5,8 @@ the reference's own fixture for config D, and the single-problem engine.
 Tolerances as for the single-problem engine: 1e-4 (max|dX| / max|X|) after a
 fixed iteration count; identical iteration counts and classifications for runs
 to convergence, W/H within 2e-3; consensus counts exact; cophenetic correlation
-within 1e-12 of the oracle evaluated on the same counts.
+within 1e-12 of the oracle evaluated on the same counts.  Problems split over
+a cluster of CTAs meet the same bars and repeat bit for bit.
 """
 from __future__ import annotations
 
@@ -124,6 +125,62 @@ def test_rank_sweep_recovers_planted_rank(pkg, synth):
     assert res.device_ms > 0
 
 
+@pytest.mark.parametrize("ctas", [1, 2, 4, 8])
+def test_cluster_split_problems(pkg, oracle, synth, ctas):
+    # Each problem on a cluster of `ctas` CTAs (rows of W split, partial sums
+    # added in rank order): fixed iterations within 1e-4 of the FP64 oracle;
+    # runs to convergence with the iteration counts and labels of one CTA per
+    # problem, W/H within 2e-3; two runs bit-identical.
+    V, _ = synth.expression_like(1500, 90, 4, seed=31)
+    n, m = V.shape
+    ranks = [2, 3, 4, 7, 11, 20]
+    seeds = [5 + r for r in ranks]
+    with pkg.Batch(n, m, ranks) as b:
+        b.set_cluster(ctas)
+        b.set_V(V)
+        b.init_random(seeds)
+        it, conv = b.run(40, 10, 1000)
+        assert b.cluster == ctas and (it == 40).all()
+        for p, (k, s) in enumerate(zip(ranks, seeds)):
+            W0, H0 = oracle.init_random(s, n, m, k)
+            Wr, Hr, _, _ = oracle.nmf(V, W0, H0, 40, 10, 1000, prec="f64")
+            assert maxnorm_rel(b.W(p), Wr) < 1e-4 and maxnorm_rel(b.H(p), Hr) < 1e-4, k
+    V, _ = synth.config_d(4)
+    n, m = V.shape
+    ranks = [3, 5, 5, 8]
+    seeds = [1, 2, 3, 4]
+    out = {}
+    for c in (1, ctas, ctas):
+        with pkg.Batch(n, m, ranks) as b:
+            b.set_cluster(c)
+            b.set_V(V)
+            b.init_random(seeds)
+            it, conv = b.run(2000, 10, 40)
+            out.setdefault(c, []).append((it, conv, b.classification(), [b.W(p) for p in range(4)],
+                                          [b.H(p) for p in range(4)]))
+    one, a, b2 = out[1][0], out[ctas][-2], out[ctas][-1]
+    assert np.array_equal(a[0], one[0]) and np.array_equal(a[1], one[1]) and np.array_equal(a[2], one[2])
+    for p in range(4):
+        assert maxnorm_rel(a[3][p], one[3][p]) < 2e-3 and maxnorm_rel(a[4][p], one[4][p]) < 2e-3
+        assert np.array_equal(a[3][p], b2[3][p]) and np.array_equal(a[4][p], b2[4][p])
+
+
+def test_cluster_with_empty_slices(pkg, oracle, synth):
+    # n = 6 rows over 8 CTAs: CTAs 6 and 7 own no rows and contribute zero partials
+    V, _ = synth.expression_like(6, 40, 2, seed=3)
+    n, m = V.shape
+    with pkg.Batch(n, m, [2, 3]) as b:
+        b.set_cluster(8)
+        b.set_V(V)
+        b.init_random([7, 8])
+        it, _ = b.run(20, 10, 1000)
+        assert (it == 20).all()
+        for p, k in enumerate((2, 3)):
+            W0, H0 = oracle.init_random(7 + p, n, m, k)
+            Wr, Hr, _, _ = oracle.nmf(V, W0, H0, 20, 10, 1000, prec="f64")
+            assert maxnorm_rel(b.W(p), Wr) < 1e-4 and maxnorm_rel(b.H(p), Hr) < 1e-4
+
+
 def test_invalid_batches(pkg):
     with pytest.raises(pkg.NMFError) as ei:
         pkg.Batch(100, 50, [2, 21])
@@ -136,3 +193,5 @@ def test_invalid_batches(pkg):
         assert ei.value.code == -5
         with pytest.raises(pkg.NMFError):
             b.set_tiles(0, 12, 16)        # wt not a multiple of 8
+        with pytest.raises(pkg.NMFError):
+            b.set_cluster(3)              # not 0, 1, 2, 4 or 8
