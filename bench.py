@@ -348,6 +348,14 @@ def serve_rates(dev, count=None, seq_sample=40):
     srv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0)
     srv.run(reqs[:8], open_loop=False)                       # warm-up (module loads, allocator pools)
     cap = srv.run(reqs, open_loop=False)
+    # the device queue (persistent serving kernel) against contexts on the
+    # requests it takes (m <= 256)
+    qsrv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
+                        batched=True)
+    small = [r for r in reqs if qsrv._queued(r)]
+    qsrv.run(small[:8], open_loop=False)
+    q_small = qsrv.run(small, open_loop=False)
+    c_small = srv.run(small, open_loop=False)
     seq = srv.run_sequential(reqs[:seq_sample])
     open_runs = {}
     for load in (SERVE["load"], 0.5):
@@ -362,6 +370,12 @@ def serve_rates(dev, count=None, seq_sample=40):
     return {"workload": SERVE["desc"], "requests": count, "value": cap.solves_per_s(), "unit": "solves/s",
             "sequential": {"value": seq.solves_per_s(), "unit": "solves/s", "sample": f"first {seq_sample} requests"},
             "speedup_vs_sequential": cap.solves_per_s() / seq.solves_per_s(),
+            "device_queue": {"requests": len(small), "max_m": qsrv.max_m, "ctas_per_request": qsrv.ctas,
+                             "value": q_small.solves_per_s(), "unit": "solves/s",
+                             "contexts_same_requests": c_small.solves_per_s(),
+                             "p50_s": q_small.latency_pct(50), "p99_s": q_small.latency_pct(99),
+                             "note": "the requests with m <= 256, all queued at t = 0: persistent serving kernel "
+                                     "vs per-request contexts"},
             "open_loop": {"arrival_rate": rate, "solves_s": op.solves_per_s(), "p50_s": op.latency_pct(50),
                           "p99_s": op.latency_pct(99), "peak_active": op.peak_active,
                           "peak_gb": op.peak_bytes / 1e9},

@@ -108,6 +108,14 @@ def load_library(path: str = LIB_PATH):
         "nmfb_batch_get_classification": ([vp, C.POINTER(u32)], i32),
         "nmfb_batch_get_WH": ([vp, u32, fp, sz, fp, sz], i32),
         "nmfb_batch_consensus": ([vp, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_double)], i32),
+        "nmfb_serve_create": ([C.POINTER(vp), i32, u32, u32, u32, u32, u32], i32),
+        "nmfb_serve_destroy": ([vp], i32),
+        "nmfb_serve_last_error": ([vp], C.c_char_p),
+        "nmfb_serve_request_bytes": ([u32, u32, u32], C.c_uint64),
+        "nmfb_serve_submit": ([vp, fp, sz, u32, u32, u32, u32, u32, u32, u32, C.POINTER(u32)], i32),
+        "nmfb_serve_poll": ([vp, u32, C.POINTER(i32)], i32),
+        "nmfb_serve_wait": ([vp, u32, C.c_double], i32),
+        "nmfb_serve_fetch": ([vp, u32, fp, sz, fp, sz, C.POINTER(u32), C.POINTER(u32), C.POINTER(i32)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -425,6 +433,89 @@ class Batch:
         self._check(self._L.nmfb_batch_consensus(self._h, k, _uptr(counts), C.byref(nruns),
                                                  C.byref(coph) if cophenetic else None))
         return counts, int(nruns.value), (coph.value if cophenetic else None)
+
+
+class Serve:
+    """Device-side request queue feeding a persistent kernel (``nmfb_serve_*``).
+
+    ``submit`` uploads a request (V: n x m float32, m <= max_m; rank k <= max_k)
+    and returns a ticket at once; clusters of ``ctas`` CTAs take requests in
+    submission order as they free up.  ``poll`` / ``wait`` / ``fetch`` collect
+    a finished request's (W, H, labels, iterations, converged).
+    """
+
+    def __init__(self, max_m: int = 256, max_k: int = 20, capacity: int = 4096, ctas: int = 4,
+                 idle_ms: int = 50, device: int = 0):
+        self._L = load_library()
+        self.max_m, self.max_k = int(max_m), int(max_k)
+        self._shapes = {}
+        self._h = C.c_void_p()
+        rc = self._L.nmfb_serve_create(C.byref(self._h), device, self.max_m, self.max_k, capacity, ctas, idle_ms)
+        if rc != NMFB_OK:
+            msg = self._L.nmfb_serve_last_error(self._h).decode() if self._h.value else "server creation failed"
+            self._L.nmfb_serve_destroy(self._h)
+            self._h = C.c_void_p()
+            raise NMFError(rc, msg)
+
+    def _check(self, rc: int):
+        if rc != NMFB_OK:
+            raise NMFError(rc, self._L.nmfb_serve_last_error(self._h).decode())
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            self._L.nmfb_serve_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def request_bytes(n: int, m: int, k: int) -> int:
+        return int(load_library().nmfb_serve_request_bytes(n, m, k))
+
+    def fits(self, m: int, k: int) -> bool:
+        return m <= self.max_m and 2 <= k <= self.max_k
+
+    def submit(self, V: np.ndarray, k: int, seed: int = 1, n_iters: int = 2000, niter_test_conv: int = 10,
+               stop_threshold: int = 40) -> int:
+        V = np.ascontiguousarray(V, np.float32)
+        n, m = V.shape
+        t = C.c_uint32()
+        self._check(self._L.nmfb_serve_submit(self._h, _fptr(V), m, n, m, k, seed, n_iters, niter_test_conv,
+                                              stop_threshold, C.byref(t)))
+        self._shapes[int(t.value)] = (n, m, int(k))
+        return int(t.value)
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int()
+        self._check(self._L.nmfb_serve_poll(self._h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout: float = 600.0):
+        self._check(self._L.nmfb_serve_wait(self._h, ticket, timeout))
+
+    def fetch(self, ticket: int):
+        """(W, H, labels, iterations, converged) of a finished request."""
+        n, m, k = self._shapes.pop(ticket)
+        W = np.empty((n, k), np.float32)
+        H = np.empty((m, k), np.float32)
+        lab = np.empty(m, np.uint32)
+        it, conv = C.c_uint32(), C.c_int()
+        rc = self._L.nmfb_serve_fetch(self._h, ticket, _fptr(W), k, _fptr(H), k, _uptr(lab), C.byref(it),
+                                      C.byref(conv))
+        if rc != NMFB_OK:
+            self._shapes[ticket] = (n, m, k)
+            self._check(rc)
+        return W, H, lab, int(it.value), bool(conv.value)
 
 
 def nmf_gpu(V: np.ndarray, k: int = 2, n_iters: int = 2000, niter_test_conv: int = 10, stop_threshold: int = 40,

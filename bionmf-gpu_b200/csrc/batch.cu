@@ -40,6 +40,9 @@
 //   colsum(W) and colsum(H) are reduced from the rows each thread just wrote,
 //   in a fixed order (warp shuffles, then warps in order).
 // Ranks 2..20 are compiled as exact-rank instantiations (no padded flops).
+// Problem inputs (V, W, H) are read through L2 only (cp.async.cg, ld.global.cg):
+// the serving kernel outlives the requests whose buffers the host frees and
+// reuses, and an SM's L1 is not coherent with copies the host makes meanwhile.
 // Tile shapes (wt, jt) are per-problem values (nmfb_batch_set_tiles; the
 // Python layer's autotuner picks them per (k, m) bucket).
 #include "nmfb_internal.cuh"
@@ -49,7 +52,11 @@
 #include <stdarg.h>
 #include <stdlib.h>
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -70,14 +77,10 @@ struct Problem {
     uint64_t ldv;
     uint32_t n, m, k, ks;
     uint32_t wt, jt;     // tile shapes
+    uint32_t n_iters, niter_test_conv, stop_threshold;   // the problem's -i, -j, -t
     uint32_t iterations; // out
     uint32_t converged;  // out
     uint32_t tests;      // out: convergence tests performed
-    uint32_t pad;
-};
-
-struct LoopArgs {
-    uint32_t n_iters, niter_test_conv, stop_threshold;
 };
 
 __host__ __device__ constexpr uint32_t ks_of(uint32_t k) { return (k + 3u) & ~3u; }
@@ -351,7 +354,7 @@ __device__ void update_W(const Problem &P, float *sm, const SmemLayout &L, bool 
         float w[K], aux[K];
 #pragma unroll
         for (int c = 0; c < K; c++) {
-            w[c] = active ? P.W[(size_t)i * KS + c] : 0.0f;
+            w[c] = active ? __ldcg(P.W + (size_t)i * KS + c) : 0.0f;
             aux[c] = 0.0f;
         }
         __syncthreads();   // the staging region may still be read by the previous phase
@@ -448,7 +451,7 @@ __device__ void classify(float *sm, const SmemLayout &L, uint32_t m, bool adjust
 }
 
 template <int K>
-__device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *s_ctl, const Slice &X)
+__device__ void run_problem(Problem &P, float *sm, uint32_t *s_ctl, const Slice &X)
 {
     constexpr uint32_t KS = ks_of(K);
     SmemLayout const L = smem_layout(P.m, KS, P.wt, P.jt, P.ldv);
@@ -461,7 +464,7 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
     {
         const float4 *src = reinterpret_cast<const float4 *>(P.H);
         float4 *dst = reinterpret_cast<float4 *>(sm + L.h);
-        for (uint32_t e = tid; e < m * KS / 4; e += NT) dst[e] = src[e];
+        for (uint32_t e = tid; e < m * KS / 4; e += NT) dst[e] = __ldcg(src + e);
     }
     for (uint32_t j = tid; j < m; j += NT) rep[j] = 0u;   // the first test compares with an all-zero vector
     if (tid < 32) first[tid] = 0xffffffffu;
@@ -476,13 +479,13 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
         for (int c = 0; c < K; c++) ws[c] = 0.0f;
         for (uint32_t i = X.r0 + tid; i < X.r1; i += NT)
 #pragma unroll
-            for (int c = 0; c < K; c++) ws[c] += P.W[(size_t)i * KS + c];
+            for (int c = 0; c < K; c++) ws[c] += __ldcg(P.W + (size_t)i * KS + c);
         __syncthreads();
         colsum_W<K>(ws, sm, L, X);
     }
 
-    uint32_t const J = A.niter_test_conv;
-    uint32_t const nblocks = A.n_iters / J, rem = A.n_iters % J;
+    uint32_t const J = P.niter_test_conv;
+    uint32_t const nblocks = P.n_iters / J, rem = P.n_iters % J;
     for (uint32_t b = 0; b < nblocks; b++) {
         for (uint32_t it = 0; it < J; it++) {
             update_H<K>(P, sm, L, X);
@@ -501,7 +504,7 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
             s_ctl[2] += 1;
             if (any)
                 s_ctl[0] = 0;
-            else if (s_ctl[0] < A.stop_threshold)
+            else if (s_ctl[0] < P.stop_threshold)
                 s_ctl[0] += 1;
             else
                 s_ctl[1] = 1;
@@ -526,13 +529,13 @@ __device__ void run_problem(Problem &P, float *sm, const LoopArgs &A, uint32_t *
     if (tid == 0) {
         P.converged = s_ctl[1];
         P.tests = s_ctl[2];
-        P.iterations = s_ctl[1] ? s_ctl[2] * J : A.n_iters;
+        P.iterations = s_ctl[1] ? s_ctl[2] * J : P.n_iters;
     }
     __syncthreads();
 }
 
 __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, const uint32_t *__restrict__ order,
-                                                 uint32_t nprob, uint32_t *__restrict__ queue, LoopArgs A)
+                                                 uint32_t nprob, uint32_t *__restrict__ queue)
 {
     extern __shared__ float4 smem4[];
     float *sm = reinterpret_cast<float *>(smem4);
@@ -560,7 +563,7 @@ __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, co
         Slice const X{crank, csize, min(P.n, crank * chunk), min(P.n, crank * chunk + chunk)};
         switch (P.k) {
 #define NMFB_BATCH_CASE(KK) \
-    case KK: run_problem<KK>(P, sm, A, s_ctl, X); break;
+    case KK: run_problem<KK>(P, sm, s_ctl, X); break;
             NMFB_BATCH_CASE(2) NMFB_BATCH_CASE(3) NMFB_BATCH_CASE(4) NMFB_BATCH_CASE(5) NMFB_BATCH_CASE(6)
             NMFB_BATCH_CASE(7) NMFB_BATCH_CASE(8) NMFB_BATCH_CASE(9) NMFB_BATCH_CASE(10) NMFB_BATCH_CASE(11)
             NMFB_BATCH_CASE(12) NMFB_BATCH_CASE(13) NMFB_BATCH_CASE(14) NMFB_BATCH_CASE(15) NMFB_BATCH_CASE(16)
@@ -573,6 +576,103 @@ __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, co
             dst->iterations = P.iterations;
             dst->converged = P.converged;
             dst->tests = P.tests;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long device_clock_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr uint32_t NO_TICKET = 0xffffffffu;
+
+// Serving: requests are published one at a time into a ring of `capacity`
+// descriptors while the kernel runs (the host copies a request's data and
+// descriptor, then the new published count, in that order on one stream).
+// A cluster's rank 0 claims the next published ticket with a compare-and-swap
+// on `taken`, waiting at most idle_ns for one; after that, or once `closing`
+// is set, the cluster leaves, and the host launches the kernel again when
+// more work is published.  Every wait is bounded by idle_ns.  A finished
+// problem's W, H and labels are in device memory before its completion record
+// (host-mapped memory) is written: iterations, converged, tests, then the
+// ticket + 1 after a system-scope fence.
+__global__ void __launch_bounds__(NT, 2) k_serve(const Problem *__restrict__ ring, uint32_t capacity,
+                                                 uint32_t *taken, const volatile uint32_t *published,
+                                                 const volatile uint32_t *closing, volatile uint32_t *done,
+                                                 unsigned long long idle_ns)
+{
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    __shared__ uint32_t s_next;
+    __shared__ uint32_t s_ctl[4];
+    cg::cluster_group const cl = cg::this_cluster();
+    uint32_t const crank = cl.block_rank(), csize = cl.num_blocks();
+    for (;;) {
+        __syncthreads();
+        if (crank == 0 && threadIdx.x == 0) {
+            uint32_t got = NO_TICKET;
+            unsigned long long const t0 = device_clock_ns();
+            for (;;) {
+                uint32_t const t = *(volatile uint32_t *)taken;
+                if (t < *published) {
+                    if (atomicCAS(taken, t, t + 1u) == t) {
+                        got = t;
+                        break;
+                    }
+                    continue;
+                }
+                if (*closing || device_clock_ns() - t0 > idle_ns) break;
+                __nanosleep(2000);
+            }
+            s_next = got;
+        }
+        uint32_t q;
+        if (csize > 1) {
+            cl.sync();
+            q = *cl.map_shared_rank(&s_next, 0u);
+            cl.sync();
+        } else {
+            __syncthreads();
+            q = s_next;
+        }
+        if (q == NO_TICKET) break;
+        uint32_t const slot = q % capacity;
+        // the descriptor was written by a host copy: read it through L2
+        Problem P;
+        {
+            const uint2 *src = reinterpret_cast<const uint2 *>(ring + slot);
+            uint2 *dst = reinterpret_cast<uint2 *>(&P);
+#pragma unroll
+            for (uint32_t w = 0; w < sizeof(Problem) / sizeof(uint2); w++) dst[w] = __ldcg(src + w);
+        }
+        uint32_t const chunk = (P.n + csize - 1) / csize;
+        Slice const X{crank, csize, min(P.n, crank * chunk), min(P.n, crank * chunk + chunk)};
+        switch (P.k) {
+#define NMFB_SERVE_CASE(KK) \
+    case KK: run_problem<KK>(P, sm, s_ctl, X); break;
+            NMFB_SERVE_CASE(2) NMFB_SERVE_CASE(3) NMFB_SERVE_CASE(4) NMFB_SERVE_CASE(5) NMFB_SERVE_CASE(6)
+            NMFB_SERVE_CASE(7) NMFB_SERVE_CASE(8) NMFB_SERVE_CASE(9) NMFB_SERVE_CASE(10) NMFB_SERVE_CASE(11)
+            NMFB_SERVE_CASE(12) NMFB_SERVE_CASE(13) NMFB_SERVE_CASE(14) NMFB_SERVE_CASE(15) NMFB_SERVE_CASE(16)
+            NMFB_SERVE_CASE(17) NMFB_SERVE_CASE(18) NMFB_SERVE_CASE(19) NMFB_SERVE_CASE(20)
+#undef NMFB_SERVE_CASE
+            default: break;
+        }
+        // every CTA's stores of W (and rank 0's of H and the labels) are done
+        __threadfence();
+        if (csize > 1)
+            cl.sync();
+        else
+            __syncthreads();
+        if (crank == 0 && threadIdx.x == 0) {
+            volatile uint32_t *rec = done + 4 * (size_t)slot;
+            rec[1] = P.iterations;
+            rec[2] = P.converged;
+            rec[3] = P.tests;
+            __threadfence_system();
+            rec[0] = q + 1u;
         }
     }
 }
@@ -1011,6 +1111,9 @@ int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, ui
     size_t smem = 0;
     for (uint32_t p = 0; p < b->nprob; p++) {
         P[p] = make_problem(b, p);
+        P[p].n_iters = n_iters;
+        P[p].niter_test_conv = niter_test_conv;
+        P[p].stop_threshold = stop_threshold;
         order[p] = p;
         smem = std::max(smem, problem_smem_bytes(b->m, b->ranks[p], b->wt[p], b->jt[p]));
     }
@@ -1047,9 +1150,8 @@ int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, ui
     uint32_t ncl = (uint32_t)nclusters < b->nprob ? (uint32_t)nclusters : b->nprob;
     cfg.gridDim = dim3(ncl * C, 1, 1);
     b->last_cluster = C;
-    LoopArgs A{n_iters, niter_test_conv, stop_threshold};
     BTRY(b, cudaEventRecord(b->ev0, b->stream));
-    BTRY(b, cudaLaunchKernelEx(&cfg, k_batch, b->dProbs, (const uint32_t *)b->dOrder, b->nprob, b->dQueue, A));
+    BTRY(b, cudaLaunchKernelEx(&cfg, k_batch, b->dProbs, (const uint32_t *)b->dOrder, b->nprob, b->dQueue));
     BTRY(b, cudaEventRecord(b->ev1, b->stream));
     BTRY(b, cudaMemcpyAsync(P.data(), b->dProbs, b->nprob * sizeof(Problem), cudaMemcpyDeviceToHost, b->stream));
     BTRY(b, cudaStreamSynchronize(b->stream));
@@ -1128,6 +1230,382 @@ int nmfb_batch_consensus(nmfb_batch *b, uint32_t k, uint32_t *counts, uint32_t *
     cudaFree(dWork);
     cudaFree(dCid);
     if (e != cudaSuccess) return bfail(b, NMFB_ECUDA, "consensus: %s", cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving: a persistent k_serve launch fed with requests as they arrive.
+namespace {
+
+constexpr uint32_t SERVE_WT = 16, SERVE_JT = 16;   // tile shapes that size the launch's shared memory
+
+// Tile shapes of a served problem: within the staging buffer the launch
+// reserves for (max_m, max_k), the tallest update_H tile (narrow problems
+// get many rows per tile: their per-tile work is small next to the staging
+// latency) and the widest update_W tile.
+void serve_tiles(uint32_t max_m, uint32_t max_k, uint32_t m, uint32_t k, uint32_t *wt, uint32_t *jt)
+{
+    uint64_t const ldmax = ((uint64_t)max_m + 31) / 32 * 32, ld = ((uint64_t)m + 31) / 32 * 32;
+    SmemLayout const Lmax = smem_layout(max_m, ks_of(max_k), SERVE_WT, SERVE_JT, ldmax);
+    uint32_t const cap = Lmax.hbuf > Lmax.wbuf ? Lmax.hbuf : Lmax.wbuf;
+    uint32_t const cs = ld < (uint64_t)NT ? (uint32_t)ld : (uint32_t)NT;
+    uint32_t w = cap / (cs + ks_of(k));
+    w = w > 512 ? 512 : (w & ~7u);
+    *wt = w < 8 ? 8 : w;
+    uint32_t j = 64;
+    while (j > 4 && (uint32_t)NT * (j + 4) > cap) j >>= 1;
+    *jt = j;
+}
+
+struct ServeSlot {
+    uint32_t ticket;      // ticket + 1 while occupied, 0 when free
+    uint32_t n, m, k;
+    float *V, *W, *H;
+    uint32_t *labels;
+};
+
+uint64_t serve_bytes(uint32_t n, uint32_t m, uint32_t k)
+{
+    uint64_t const ldv = ((uint64_t)m + 31) / 32 * 32, ks = ks_of(k);
+    return ((uint64_t)n * ldv + (uint64_t)n * ks + (uint64_t)m * ks + m) * 4u + 4 * 256u;
+}
+
+}  // namespace
+
+struct nmfb_serve {
+    int device;
+    uint32_t max_m, max_k, capacity, ctas, nclusters;
+    unsigned long long idle_ns;
+    size_t smem;
+    cudaStream_t kstream, cstream, rstream;   // kernel, uploads, results
+    cudaMemPool_t pool;
+    Problem *dRing, *hRing;                   // descriptors (device) and their pinned host copies
+    uint32_t *dCtl;                           // [0] taken, [32] published
+    uint32_t *hPub;                           // pinned: published value per slot (ticket + 1)
+    volatile uint32_t *hClosing;              // mapped: set by destroy
+    volatile uint32_t *hDone;                 // mapped: completion records, 4 words per slot
+    uint32_t *dClosingAlias, *dDoneAlias;
+    cudaEvent_t kdone;
+    bool running;
+    uint32_t next_ticket, published;
+    std::vector<ServeSlot> slots;
+    std::mutex mu;
+    char err[512];
+};
+
+static int sfail(nmfb_serve *s, int code, const char *fmt, ...)
+{
+    if (s) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(s->err, sizeof(s->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define STRY(s, call)                                                                                      \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return sfail((s), NMFB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+// Launch k_serve if it is not running and published work is untaken (caller holds mu).
+static int serve_ensure_running(nmfb_serve *s)
+{
+    if (s->running) {
+        cudaError_t const q = cudaEventQuery(s->kdone);
+        if (q == cudaErrorNotReady) return NMFB_OK;
+        if (q != cudaSuccess) return sfail(s, NMFB_ECUDA, "serving kernel: %s", cudaGetErrorString(q));
+        s->running = false;
+    }
+    uint32_t taken = 0;
+    STRY(s, cudaMemcpyAsync(&taken, s->dCtl, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->kstream));
+    STRY(s, cudaStreamSynchronize(s->kstream));
+    if (taken >= s->published) return NMFB_OK;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = s->ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(s->nclusters * s->ctas, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = s->smem;
+    cfg.stream = s->kstream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    STRY(s, cudaLaunchKernelEx(&cfg, k_serve, (const Problem *)s->dRing, s->capacity, s->dCtl,
+                               (const volatile uint32_t *)(s->dCtl + 32), (const volatile uint32_t *)s->dClosingAlias,
+                               (volatile uint32_t *)s->dDoneAlias, s->idle_ns));
+    STRY(s, cudaEventRecord(s->kdone, s->kstream));
+    s->running = true;
+    return NMFB_OK;
+}
+
+extern "C" {
+
+uint64_t nmfb_serve_request_bytes(uint32_t n, uint32_t m, uint32_t k) { return serve_bytes(n, m, k); }
+
+int nmfb_serve_create(nmfb_serve **out, int device, uint32_t max_m, uint32_t max_k, uint32_t capacity,
+                      uint32_t ctas, uint32_t idle_ms)
+{
+    if (!out) return NMFB_EINVAL;
+    *out = nullptr;
+    nmfb_serve *s = new (std::nothrow) nmfb_serve();
+    if (!s) return NMFB_ENOMEM;
+    *out = s;
+    s->device = device;
+    if (max_m < 2 || max_k < KMIN || max_k > KMAX || capacity == 0 || capacity > (1u << 20) ||
+        (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8) || idle_ms == 0)
+        return sfail(s, NMFB_EINVAL, "serve: max_m >= 2, max_k in [2, 20], capacity in [1, 2^20], ctas 1/2/4/8, idle > 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return sfail(s, NMFB_ENODEV, "no CUDA device %d", device);
+    }
+    int major = 0, sms = 0, optin = 0;
+    STRY(s, cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) return sfail(s, NMFB_ENODEV, "device %d is not sm_100a", device);
+    STRY(s, cudaSetDevice(device));
+    STRY(s, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    STRY(s, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    s->max_m = max_m;
+    s->max_k = max_k;
+    s->capacity = capacity;
+    s->ctas = ctas;
+    s->idle_ns = (unsigned long long)idle_ms * 1000000ull;
+    s->smem = problem_smem_bytes(max_m, max_k, SERVE_WT, SERVE_JT);
+    if (s->smem + 64 > (size_t)optin)
+        return sfail(s, NMFB_EINVAL, "serve: max_m = %u with max_k = %u does not fit shared memory", max_m, max_k);
+    STRY(s, cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+    {
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ctas * (uint32_t)sms, 1, 1);
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.dynamicSmemBytes = s->smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        STRY(s, cudaOccupancyMaxActiveClusters(&ncl, k_serve, &cfg));
+        if (ncl < 1) return sfail(s, NMFB_EINVAL, "serve: no cluster of %u CTAs fits", ctas);
+        s->nclusters = (uint32_t)ncl;
+    }
+    STRY(s, cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking));
+    STRY(s, cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
+    STRY(s, cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking));
+    STRY(s, cudaEventCreateWithFlags(&s->kdone, cudaEventDisableTiming));
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    STRY(s, cudaMemPoolCreate(&s->pool, &props));
+    uint64_t keep = UINT64_MAX;
+    STRY(s, cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    STRY(s, cudaMalloc(&s->dRing, (size_t)capacity * sizeof(Problem)));
+    STRY(s, cudaMalloc(&s->dCtl, 64 * sizeof(uint32_t)));
+    STRY(s, cudaMemset(s->dCtl, 0, 64 * sizeof(uint32_t)));
+    STRY(s, cudaMallocHost(&s->hRing, (size_t)capacity * sizeof(Problem)));
+    STRY(s, cudaMallocHost(&s->hPub, (size_t)capacity * sizeof(uint32_t)));
+    void *p = nullptr;
+    STRY(s, cudaHostAlloc(&p, sizeof(uint32_t), cudaHostAllocMapped));
+    s->hClosing = (volatile uint32_t *)p;
+    *s->hClosing = 0;
+    STRY(s, cudaHostGetDevicePointer((void **)&s->dClosingAlias, p, 0));
+    STRY(s, cudaHostAlloc(&p, (size_t)capacity * 4 * sizeof(uint32_t), cudaHostAllocMapped));
+    memset(p, 0, (size_t)capacity * 4 * sizeof(uint32_t));
+    s->hDone = (volatile uint32_t *)p;
+    STRY(s, cudaHostGetDevicePointer((void **)&s->dDoneAlias, p, 0));
+    s->slots.assign(capacity, ServeSlot{});
+    return NMFB_OK;
+}
+
+int nmfb_serve_destroy(nmfb_serve *s)
+{
+    if (!s) return NMFB_OK;
+    cudaSetDevice(s->device);
+    if (s->hClosing) *s->hClosing = 1;
+    if (s->kstream) cudaStreamSynchronize(s->kstream);
+    if (s->cstream) cudaStreamSynchronize(s->cstream);
+    if (s->rstream) cudaStreamSynchronize(s->rstream);
+    for (ServeSlot &sl : s->slots)
+        if (sl.ticket) {
+            cudaFree(sl.V);
+            cudaFree(sl.W);
+            cudaFree(sl.H);
+            cudaFree(sl.labels);
+        }
+    if (s->dRing) cudaFree(s->dRing);
+    if (s->dCtl) cudaFree(s->dCtl);
+    if (s->hRing) cudaFreeHost(s->hRing);
+    if (s->hPub) cudaFreeHost(s->hPub);
+    if (s->hClosing) cudaFreeHost((void *)s->hClosing);
+    if (s->hDone) cudaFreeHost((void *)s->hDone);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->kdone) cudaEventDestroy(s->kdone);
+    if (s->kstream) cudaStreamDestroy(s->kstream);
+    if (s->cstream) cudaStreamDestroy(s->cstream);
+    if (s->rstream) cudaStreamDestroy(s->rstream);
+    delete s;
+    return NMFB_OK;
+}
+
+const char *nmfb_serve_last_error(const nmfb_serve *s) { return s ? s->err : "null server"; }
+
+int nmfb_serve_submit(nmfb_serve *s, const float *V, size_t ldv, uint32_t n, uint32_t m, uint32_t k, uint32_t seed,
+                      uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold, uint32_t *ticket)
+{
+    if (!s || !V || !ticket) return sfail(s, NMFB_EINVAL, "nmfb_serve_submit: null argument");
+    if (n < 2 || m < 2 || m > s->max_m || ldv < m || k < KMIN || k > s->max_k || k > (n < m ? n : m))
+        return sfail(s, NMFB_EINVAL, "request %u x %u, k = %u outside the server's limits (m <= %u, 2 <= k <= min(%u, n, m))",
+                     n, m, k, s->max_m, s->max_k);
+    if (n_iters == 0 || niter_test_conv == 0 || stop_threshold == 0)
+        return sfail(s, NMFB_EINVAL, "nIters, niter_test_conv and stop_threshold must be positive");
+    {
+        uint32_t wt, jt;
+        serve_tiles(s->max_m, s->max_k, m, k, &wt, &jt);
+        if (problem_smem_bytes(m, k, wt, jt) > s->smem)
+            return sfail(s, NMFB_EINVAL, "request %u x %u, k = %u: tiles exceed the server's shared memory", n, m, k);
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    STRY(s, cudaSetDevice(s->device));
+    uint32_t const t = s->next_ticket, slot = t % s->capacity;
+    ServeSlot &sl = s->slots[slot];
+    if (sl.ticket) return sfail(s, NMFB_ESTATE, "all %u request slots are in use (fetch finished requests first)", s->capacity);
+    uint32_t const ks = ks_of(k);
+    uint64_t const ldp = ((uint64_t)m + 31) / 32 * 32;
+    // CPU_RANDOM initialisation (src/NMF_routines.c:299-307), as nmfb_init_random
+    std::vector<float> W((size_t)n * ks), H((size_t)m * ks);
+    {
+        char rstate[128];
+        struct random_data rd;
+        memset(&rd, 0, sizeof(rd));
+        initstate_r(seed, rstate, sizeof(rstate), &rd);
+        auto next = [&]() -> float {
+            int32_t r;
+            random_r(&rd, &r);
+            return ((float)r) / ((float)RAND_MAX) + FLT_MIN;
+        };
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t c = 0; c < ks; c++) W[(size_t)i * ks + c] = (c < k) ? next() : 0.0f;
+        for (uint32_t j = 0; j < m; j++)
+            for (uint32_t c = 0; c < ks; c++) H[(size_t)j * ks + c] = (c < k) ? next() : 0.0f;
+    }
+    ServeSlot ns{};
+    cudaError_t e = cudaMallocFromPoolAsync((void **)&ns.V, (size_t)n * ldp * sizeof(float), s->pool, s->cstream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&ns.W, W.size() * sizeof(float), s->pool, s->cstream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&ns.H, H.size() * sizeof(float), s->pool, s->cstream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&ns.labels, (size_t)m * sizeof(uint32_t), s->pool, s->cstream);
+    if (e != cudaSuccess) {
+        if (ns.V) cudaFreeAsync(ns.V, s->cstream);
+        if (ns.W) cudaFreeAsync(ns.W, s->cstream);
+        if (ns.H) cudaFreeAsync(ns.H, s->cstream);
+        cudaGetLastError();
+        return sfail(s, NMFB_ENOMEM, "request memory: %s", cudaGetErrorString(e));
+    }
+    STRY(s, cudaMemsetAsync(ns.V, 0, (size_t)n * ldp * sizeof(float), s->cstream));
+    STRY(s, cudaMemcpy2DAsync(ns.V, ldp * sizeof(float), V, ldv * sizeof(float), m * sizeof(float), n,
+                              cudaMemcpyDefault, s->cstream));
+    STRY(s, cudaMemcpyAsync(ns.W, W.data(), W.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+    STRY(s, cudaMemcpyAsync(ns.H, H.data(), H.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+    Problem &P = s->hRing[slot];
+    memset(&P, 0, sizeof(P));
+    P.V = ns.V;
+    P.W = ns.W;
+    P.H = ns.H;
+    P.labels = ns.labels;
+    P.ldv = ldp;
+    P.n = n;
+    P.m = m;
+    P.k = k;
+    P.ks = ks;
+    serve_tiles(s->max_m, s->max_k, m, k, &P.wt, &P.jt);
+    P.n_iters = n_iters;
+    P.niter_test_conv = niter_test_conv;
+    P.stop_threshold = stop_threshold;
+    STRY(s, cudaMemcpyAsync(s->dRing + slot, &P, sizeof(Problem), cudaMemcpyHostToDevice, s->cstream));
+    s->hDone[4 * (size_t)slot] = 0;
+    // the new published count follows the request's data on the same stream
+    s->hPub[slot] = t + 1u;
+    STRY(s, cudaMemcpyAsync(s->dCtl + 32, &s->hPub[slot], sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
+    // the pageable W / H copies have been staged when they return; the staging
+    // vectors may go
+    ns.ticket = t + 1u;
+    ns.n = n;
+    ns.m = m;
+    ns.k = k;
+    sl = ns;
+    s->next_ticket = t + 1u;
+    s->published = t + 1u;
+    *ticket = t;
+    return serve_ensure_running(s);
+}
+
+int nmfb_serve_poll(nmfb_serve *s, uint32_t ticket, int *done)
+{
+    if (!s || !done) return NMFB_EINVAL;
+    uint32_t const slot = ticket % s->capacity;
+    if (s->slots[slot].ticket != ticket + 1u) return sfail(s, NMFB_EINVAL, "ticket %u is not pending", ticket);
+    *done = (s->hDone[4 * (size_t)slot] == ticket + 1u) ? 1 : 0;
+    if (*done) {
+        std::atomic_thread_fence(std::memory_order_acquire);
+        return NMFB_OK;
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    STRY(s, cudaSetDevice(s->device));
+    return serve_ensure_running(s);
+}
+
+int nmfb_serve_wait(nmfb_serve *s, uint32_t ticket, double timeout_s)
+{
+    auto const t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        int done = 0;
+        int const rc = nmfb_serve_poll(s, ticket, &done);
+        if (rc != NMFB_OK || done) return rc;
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s)
+            return sfail(s, NMFB_ETIMEOUT, "request %u not finished after %.1f s", ticket, timeout_s);
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+}
+
+int nmfb_serve_fetch(nmfb_serve *s, uint32_t ticket, float *W, size_t ldw, float *H, size_t ldh, uint32_t *labels,
+                     uint32_t *iterations, int *converged)
+{
+    if (!s) return NMFB_EINVAL;
+    int done = 0;
+    int rc = nmfb_serve_poll(s, ticket, &done);
+    if (rc) return rc;
+    if (!done) return sfail(s, NMFB_ESTATE, "request %u has not finished", ticket);
+    uint32_t const slot = ticket % s->capacity;
+    std::lock_guard<std::mutex> lock(s->mu);
+    STRY(s, cudaSetDevice(s->device));
+    ServeSlot &sl = s->slots[slot];
+    uint32_t const ks = ks_of(sl.k);
+    if ((W && ldw < sl.k) || (H && ldh < sl.k)) return sfail(s, NMFB_EINVAL, "leading dimension below k");
+    if (W)
+        STRY(s, cudaMemcpy2DAsync(W, ldw * sizeof(float), sl.W, ks * sizeof(float), sl.k * sizeof(float), sl.n,
+                                  cudaMemcpyDeviceToHost, s->rstream));
+    if (H)
+        STRY(s, cudaMemcpy2DAsync(H, ldh * sizeof(float), sl.H, ks * sizeof(float), sl.k * sizeof(float), sl.m,
+                                  cudaMemcpyDeviceToHost, s->rstream));
+    if (labels)
+        STRY(s, cudaMemcpyAsync(labels, sl.labels, (size_t)sl.m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->rstream));
+    STRY(s, cudaStreamSynchronize(s->rstream));
+    if (iterations) *iterations = s->hDone[4 * (size_t)slot + 1];
+    if (converged) *converged = (int)s->hDone[4 * (size_t)slot + 2];
+    STRY(s, cudaFreeAsync(sl.V, s->rstream));
+    STRY(s, cudaFreeAsync(sl.W, s->rstream));
+    STRY(s, cudaFreeAsync(sl.H, s->rstream));
+    STRY(s, cudaFreeAsync(sl.labels, s->rstream));
+    sl = ServeSlot{};
     return NMFB_OK;
 }
 

@@ -2,19 +2,23 @@
 
 A request carries its own V (host memory), rank k, seed and stopping rules
 (-i / -j / -t).  The server admits requests in arrival order while their
-device memory (``context_bytes``, an upper bound of what the context
-allocates) fits the HBM budget and a worker is free; each admitted request
-gets its own context on its own CUDA stream, keeps V, W and H resident on the
-device for its whole solve, and runs the reference's loop (``NMF.run``).  The
-workers are host threads: the C ABI releases the interpreter lock, so the
-contexts' kernels are queued concurrently and overlap on the device, and a
-request that arrives while others run starts as soon as memory and a worker
-free up (continuous admission; no request waits for a whole batch to drain).
+device memory fits the HBM budget, and runs each on one of two paths:
 
-Every kernel of a context sums in a fixed order that depends only on the
-request's own sizes, so a request's result is the same alone and in any mix.
-Context memory is stream-ordered (cudaMallocAsync), so creating and freeing
-contexts does not stall the others.
+* requests whose H fits a CTA's shared memory (m <= max_m, k <= 20) go to the
+  device queue (``Serve``, ``nmfb_serve_*``): the admission thread uploads V
+  and queues the request, a persistent kernel's clusters of CTAs take queued
+  requests as they free up and run the reference's loop on them, and a
+  collector thread fetches finished ones.  Requests that arrive while others
+  are on the GPU join the running kernel (continuous batching); no launch per
+  iteration or per request;
+* larger requests get their own context on their own CUDA stream (V, W, H
+  resident for the whole solve, ``NMF.run``), driven by worker threads (the C
+  ABI releases the interpreter lock, so the contexts' kernels overlap).
+
+Both paths sum in a fixed order that depends only on the request's own sizes,
+so a request's result is the same alone and in any mix.  Device memory of
+both paths is stream-ordered, so admitting and retiring requests does not
+stall the others.
 """
 from __future__ import annotations
 
@@ -25,7 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import NMF, NMFError, context_bytes  # noqa: F401
+from . import NMF, NMFError, Serve, context_bytes  # noqa: F401
 
 
 @dataclass
@@ -72,16 +76,35 @@ class ServeStats:
 
 
 class Server:
-    """Admission by device-memory budget and worker count, FIFO order."""
+    """Admission by device-memory budget (and, for the context path, worker
+    count), FIFO order.  batched=True sends requests that fit (m <= max_m,
+    k <= 20) to the device queue.  It is off by default: on one GPU the
+    persistent serving CTAs (two per SM) and the fused kernels of the context
+    path cannot share an SM, so in a mixed stream each path waits for the
+    other's SMs (measured: a mix served both ways ran slower than with
+    contexts alone)."""
 
-    def __init__(self, budget_bytes: float = 120e9, workers: int = 16, arm: str = "fused", device: int = 0):
+    def __init__(self, budget_bytes: float = 120e9, workers: int = 16, arm: str = "fused", device: int = 0,
+                 batched: bool = False, max_m: int = 256, ctas: int = 4):
         self.budget = int(budget_bytes)
         self.workers = int(workers)
         self.arm = arm
         self.device = device
+        self.batched = batched
+        self.max_m = int(max_m)
+        self.ctas = int(ctas)
 
     def _arm_for(self, k: int) -> str:
         return self.arm if k <= 64 else "plain"
+
+    def _queued(self, r: Request) -> bool:
+        return self.batched and r.V.shape[1] <= self.max_m and 2 <= r.k <= 20
+
+    def _bytes(self, r: Request) -> int:
+        n, m = r.V.shape
+        if self._queued(r):
+            return Serve.request_bytes(n, m, r.k)
+        return context_bytes(n, m, r.k, self._arm_for(r.k), self.device)
 
     def _solve(self, req: Request, t0: float, admitted: float) -> Result:
         n, m = req.V.shape
@@ -96,47 +119,110 @@ class Server:
         """Serve `requests` (sorted by arrival).  open_loop: each request is
         released at its arrival time; otherwise all are available at t = 0."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        need = [context_bytes(r.V.shape[0], r.V.shape[1], r.k, self._arm_for(r.k), self.device) for r in reqs]
+        need = [self._bytes(r) for r in reqs]
         for r, b in zip(reqs, need):
             if b > self.budget:
                 raise NMFError(-3, f"request {r.rid} needs {b} bytes, more than the {self.budget}-byte budget")
         stats = ServeStats()
         lock = threading.Condition()
-        state = {"bytes": 0, "active": 0}
-        futures = []
+        state = {"bytes": 0, "active": 0, "workers": 0, "admitting": True}
+        futures, pending, queued_results = [], {}, []
+        q = Serve(max_m=self.max_m, ctas=self.ctas, device=self.device) if self.batched else None
 
-        def finish(b):
+        def finish(b, worker):
             with lock:
                 state["bytes"] -= b
                 state["active"] -= 1
+                if worker:
+                    state["workers"] -= 1
                 lock.notify_all()
 
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=self.workers) as pool:
-            for r, b in zip(reqs, need):
-                if open_loop:
-                    wait = r.arrival - (time.perf_counter() - t0)
-                    if wait > 0:
-                        time.sleep(wait)
+
+        errors = []
+
+        def collect():
+            try:
+                collect_loop()
+            except BaseException as exc:   # surfaced by the admission loop and after the join
                 with lock:
-                    while state["bytes"] + b > self.budget or state["active"] >= self.workers:
-                        lock.wait()
-                    state["bytes"] += b
-                    state["active"] += 1
-                    stats.peak_bytes = max(stats.peak_bytes, state["bytes"])
-                    stats.peak_active = max(stats.peak_active, state["active"])
-                admitted = time.perf_counter() - t0
-                if not open_loop:
-                    r = Request(r.V, r.k, r.seed, r.n_iters, r.niter_test_conv, r.stop_threshold, 0.0, r.rid)
+                    errors.append(exc)
+                    lock.notify_all()
 
-                def job(r=r, b=b, admitted=admitted):
-                    try:
-                        return self._solve(r, t0, admitted)
-                    finally:
-                        finish(b)
+        def collect_loop():
+            # fetch finished queued requests until admission is over and none is pending
+            while True:
+                with lock:
+                    if not state["admitting"] and not pending:
+                        return
+                    items = list(pending.items())
+                got = False
+                for ticket, (r, b, admitted) in items:
+                    if q.poll(ticket):
+                        W, H, _, it, conv = q.fetch(ticket)
+                        queued_results.append(Result(r.rid, W, H, it, conv, r.arrival, admitted,
+                                                     time.perf_counter() - t0))
+                        with lock:
+                            del pending[ticket]
+                        finish(b, False)
+                        got = True
+                if not got:
+                    time.sleep(1e-4)
 
-                futures.append(pool.submit(job))
-            stats.results = [f.result() for f in futures]
+        collector = threading.Thread(target=collect, daemon=True) if q else None
+        if collector:
+            collector.start()
+        try:
+            with ThreadPoolExecutor(max_workers=self.workers) as pool:
+                for r, b in zip(reqs, need):
+                    if open_loop:
+                        wait = r.arrival - (time.perf_counter() - t0)
+                        if wait > 0:
+                            time.sleep(wait)
+                    queued = q is not None and self._queued(r)
+                    with lock:
+                        while not errors and (state["bytes"] + b > self.budget or
+                                              (not queued and state["workers"] >= self.workers)):
+                            lock.wait()
+                        if errors:
+                            raise errors[0]
+                        state["bytes"] += b
+                        state["active"] += 1
+                        if not queued:
+                            state["workers"] += 1
+                        stats.peak_bytes = max(stats.peak_bytes, state["bytes"])
+                        stats.peak_active = max(stats.peak_active, state["active"])
+                    admitted = time.perf_counter() - t0
+                    if not open_loop:
+                        r = Request(r.V, r.k, r.seed, r.n_iters, r.niter_test_conv, r.stop_threshold, 0.0, r.rid)
+                    if queued:
+                        ticket = q.submit(r.V, r.k, r.seed, r.n_iters, r.niter_test_conv, r.stop_threshold)
+                        with lock:
+                            pending[ticket] = (r, b, admitted)
+                        continue
+
+                    def job(r=r, b=b, admitted=admitted):
+                        try:
+                            return self._solve(r, t0, admitted)
+                        finally:
+                            finish(b, True)
+
+                    futures.append(pool.submit(job))
+                with lock:
+                    state["admitting"] = False
+                stats.results = [f.result() for f in futures]
+            if collector:
+                collector.join()
+            if errors:
+                raise errors[0]
+            stats.results += queued_results
+        finally:
+            with lock:
+                state["admitting"] = False
+                if collector and collector.is_alive():
+                    pending.clear()
+            if q:
+                q.close()
         stats.wall_s = time.perf_counter() - t0
         return stats
 

@@ -248,6 +248,41 @@ int nmfb_batch_get_WH(nmfb_batch *b, uint32_t p, float *W, size_t ldw, float *H,
 int nmfb_batch_consensus(nmfb_batch *b, uint32_t k, uint32_t *counts, uint32_t *nruns, double *cophenetic);
 
 /* ---------------------------------------------------------------------------
+ * Serving (no counterpart in the reference, which solves one matrix per
+ * process): requests with their own V (n x m, m <= max_m), rank k (2..max_k,
+ * at most 20), seed and -i/-j/-t are queued on the device while a persistent
+ * kernel runs; clusters of `ctas` CTAs take them in submission order as they
+ * free up, so a request that arrives while others run starts as soon as a
+ * cluster is free, and runs the reference's loop exactly as the batched
+ * engine does (a request's result does not depend on what else is queued).
+ * The kernel leaves after idle_ms without work and is launched again by the
+ * next submit or poll.  Device memory per request: nmfb_serve_request_bytes,
+ * taken from a pool owned by the server when the request is submitted and
+ * returned by nmfb_serve_fetch.  One thread may submit while others poll,
+ * wait and fetch; each ticket is polled and fetched by one thread.
+ */
+typedef struct nmfb_serve nmfb_serve;
+
+int nmfb_serve_create(nmfb_serve **s, int device, uint32_t max_m, uint32_t max_k, uint32_t capacity, uint32_t ctas,
+                      uint32_t idle_ms);
+int nmfb_serve_destroy(nmfb_serve *s);
+const char *nmfb_serve_last_error(const nmfb_serve *s);
+uint64_t nmfb_serve_request_bytes(uint32_t n, uint32_t m, uint32_t k);
+
+/* Uploads V (host or device pointer, leading dimension ldv), initialises W and
+ * H as nmfb_init_random(seed) does, and queues the request; *ticket identifies
+ * it.  NMFB_ESTATE when `capacity` requests are already queued or unfetched. */
+int nmfb_serve_submit(nmfb_serve *s, const float *V, size_t ldv, uint32_t n, uint32_t m, uint32_t k, uint32_t seed,
+                      uint32_t n_iters, uint32_t niter_test_conv, uint32_t stop_threshold, uint32_t *ticket);
+int nmfb_serve_poll(nmfb_serve *s, uint32_t ticket, int *done);
+int nmfb_serve_wait(nmfb_serve *s, uint32_t ticket, double timeout_s);   /* NMFB_ETIMEOUT after timeout_s */
+
+/* Copies a finished request's W (n x k), H (m x k) and labels (m); any may be
+ * NULL.  Frees the request's device memory and its ticket. */
+int nmfb_serve_fetch(nmfb_serve *s, uint32_t ticket, float *W, size_t ldw, float *H, size_t ldh, uint32_t *labels,
+                     uint32_t *iterations, int *converged);
+
+/* ---------------------------------------------------------------------------
  * update_H without any allocation.  No counterpart in the reference: it is an
  * addition of this library for callers that must not allocate device memory,
  * such as a host framework whose caching allocator already owns the HBM, a
