@@ -605,6 +605,7 @@ def main():
     ap.add_argument("--batch-wave", type=int, default=0, metavar="K",
                     help="profiling case of the batched kernel: one wave (2 per SM) of rank-K problems of the "
                          "sweep matrix, 20 iterations, run twice; prints the device times")
+    ap.add_argument("--batch-ctas", type=int, default=0, help="CTAs per problem for --batch-wave (0 = automatic)")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -620,10 +621,11 @@ def main():
         with pkg.Batch(V.shape[0], V.shape[1], [a.batch_wave] * nprob) as b:
             b.set_V(V)
             b.init_random(np.arange(1, nprob + 1, dtype=np.uint32))
+            b.set_cluster(a.batch_ctas)
             for rep in range(2):
                 b.run(20, 20, 1 << 30)
                 print(json.dumps({"batch_wave_k": a.batch_wave, "problems": nprob, "iterations": 20,
-                                  "device_ms": b.last_ms()}), flush=True)
+                                  "ctas_per_problem": b.cluster, "device_ms": b.last_ms()}), flush=True)
         return
     if world > 1:
         import datetime
