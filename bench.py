@@ -385,6 +385,43 @@ def serve_rates(dev, count=None, seq_sample=40):
             "workers": SERVE["workers"]}
 
 
+SERVE_SMALL = {"requests": 400, "n": (500, 5000), "m": (20, 256), "k": (2, 10), "iters": 300,
+               "desc": "requests n~U[500,5000], m~logU[20,256], k~U[2,10], planted Poisson V, 300-iteration cap, "
+                       "all queued at t = 0"}
+
+
+def serve_small_rates(dev, seq_sample=40):
+    """Many small requests (the regime the device queue is for): the
+    persistent serving kernel against per-request contexts (concurrent, 32
+    workers) and one request at a time."""
+    _import_package()
+    import nmf_b200.serve as serve
+    import nmf_b200.synth as synth
+    rng = np.random.default_rng(23)
+    reqs = []
+    for i in range(SERVE_SMALL["requests"]):
+        n = int(rng.integers(SERVE_SMALL["n"][0], SERVE_SMALL["n"][1] + 1))
+        m = int(np.exp(rng.uniform(np.log(SERVE_SMALL["m"][0]), np.log(SERVE_SMALL["m"][1]))))
+        k = min(int(rng.integers(SERVE_SMALL["k"][0], SERVE_SMALL["k"][1] + 1)), m)
+        V, _ = synth.poisson_counts(n, m, k, 5000 + i)
+        reqs.append(serve.Request(V, k, seed=1 + i, n_iters=SERVE_SMALL["iters"], niter_test_conv=10,
+                                  stop_threshold=40, rid=i))
+    q = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
+                     batched=True)
+    c = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0)
+    q.run(reqs[:8], open_loop=False)
+    c.run(reqs[:8], open_loop=False)
+    qs = q.run(reqs, open_loop=False)
+    cs = c.run(reqs, open_loop=False)
+    seq = c.run_sequential(reqs[:seq_sample])
+    return {"workload": SERVE_SMALL["desc"], "requests": len(reqs), "unit": "solves/s",
+            "device_queue": {"value": qs.solves_per_s(), "p50_s": qs.latency_pct(50), "p99_s": qs.latency_pct(99)},
+            "contexts": {"value": cs.solves_per_s(), "p50_s": cs.latency_pct(50), "p99_s": cs.latency_pct(99)},
+            "sequential": {"value": seq.solves_per_s(), "sample": f"first {seq_sample} requests"},
+            "queue_vs_contexts": qs.solves_per_s() / cs.solves_per_s(),
+            "queue_vs_sequential": qs.solves_per_s() / seq.solves_per_s()}
+
+
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -405,6 +442,20 @@ def run_reference_arm(a, rank, world):
             "cpu_baseline": r, "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0,
                                        "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def replica_rate(ms, units_per_rank, world, device="cpu"):
+    """Whole-job rate of `world` independent replicas (one per GPU): each rank
+    processed `units_per_rank` in its own device time `ms`; the job's time is
+    the slowest rank's (all-reduce MAX over the process group).  Returns
+    (ms_max, units per second of the whole job)."""
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return ms_max, units_per_rank * world / (ms_max / 1e3)
 
 
 def run_engine_arm(a, rank, world, local_rank):
@@ -451,12 +502,7 @@ def run_engine_arm(a, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    iters_total = a.steps * J * world
-    value = iters_total / (ms_max / 1e3)
+    ms_max, value = replica_rate(ms, a.steps * J, world, dev)
 
     # roofline of the dominant kernel: V read once per launch (n*m*4 bytes).
     cls = 0 if prof[0][0] >= prof[1][0] else 1
@@ -504,15 +550,23 @@ def run_engine_arm(a, rank, world, local_rank):
     e.close()
     extras = {}
     if rank == 0 and world == 1 and not a.no_extras:
+        def guarded(fn, *args):
+            # an extra measurement that fails is reported, not fatal to the line
+            try:
+                return fn(*args)
+            except Exception as exc:
+                return {"error": f"{type(exc).__name__}: {exc}"}
+
         extras["plain_arm"] = plain_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm)
         extras["plain_arm"]["fused_speedup"] = value / extras["plain_arm"]["value"]
-        extras["arms"] = {arm: other_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, arm)
+        extras["arms"] = {arm: guarded(other_arm_rate, a, pkg, V, dev, stream, n, m, k, hbm, arm)
                           for arm in ("bf16x3", "split_bf16", "bf16", "fused_tf32")}
         del V
         torch.cuda.empty_cache()
-        extras["sweep"] = sweep_rates(dev)
-        extras["streamed"] = stream_rates(dev)
-        extras["serving"] = serve_rates(dev)
+        extras["sweep"] = guarded(sweep_rates, dev)
+        extras["streamed"] = guarded(stream_rates, dev)
+        extras["serving"] = guarded(serve_rates, dev)
+        extras["serving_small"] = guarded(serve_small_rates, dev)
     if rank != 0:
         return
     line = {"metric": "KL-NMF iterations/s", "value": value, "unit": "iters/s", "n_gpus": world,
