@@ -19,9 +19,14 @@ rank-selection sweep 5000 x 200, k = 2..10 x 50 restarts, as one persistent
 launch: solves/s on the device and end to end, against the same solves run
 one by one through the single-problem engine).
 
+Further extras: ``workloads`` (the fused arm at 60000 x 5000 k = 64 and at
+20000 x 1000 k = 16) and ``reference_cuda`` (the reference's own CUDA build,
+oracle/_ref/NMF_GPU compiled from its sources, timed on the same GPU and the
+same matrices: a baseline leg, like ``cpu_baseline``, never the product).
+
 ``--impl reference`` times the CPU restatement of the reference's loop
-(oracle/, OpenMP, all host threads) on a bounded row sample of the same
-workload, scaled to the full matrix.
+(oracle/, OpenMP, all host threads) on the same full matrix, each step the
+engine's step (10 iterations + adjust + classification); nothing is scaled.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 Under torchrun (N > 1) every rank runs an independent replica (weak scaling).
@@ -92,25 +97,73 @@ def ncu_traffic(kernel_key: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clocks and throttle reasons of one GPU, sampled every 10 ms by an NVML
+    thread (the GPU is found by its PCI bus id, so CUDA_VISIBLE_DEVICES
+    renumbering does not matter); nvidia-smi every 100 ms where NVML is
+    unavailable.  `mark(True/False)` brackets the timed region, whose samples
+    are summarised separately from the whole window."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.01):
         self.index = index
+        self.period = period_s
+        self.samples = []          # (t, sm_mhz, reasons bitmask)
+        self.window = [None, None]
         self.proc = None
+        self.thread = None
+        self.max_mhz = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.index)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def __enter__(self):
-        if shutil.which("nvidia-smi"):
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+
+            def loop():
+                while not self.stop.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), float(sm), int(rs)))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            self.source = "nvml, 10 ms"
+        except Exception:
+            if shutil.which("nvidia-smi"):
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi, 100 ms"
         return self
+
+    def mark(self, begin: bool):
+        self.window[0 if begin else 1] = time.perf_counter()
 
     def __exit__(self, *exc):
         self.out = ""
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -118,7 +171,25 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
+    def _summ(self, rows):
+        if not rows:
+            return None
+        sm = [r[1] for r in rows]
+        reasons = sorted({name for r in rows for name, bit in self.REASONS.items() if r[2] & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm), "reasons": reasons, "samples": len(rows)}
+
     def summary(self):
+        if self.thread:
+            t0, t1 = self.window
+            inside = [r for r in self.samples if t0 is not None and t1 is not None and t0 <= r[0] <= t1]
+            whole = self._summ(self.samples) or {"sm_mhz": None, "reasons": ["no samples"], "samples": 0}
+            timed = self._summ(inside)
+            out = dict(whole)
+            out["sm_max_mhz"] = self.max_mhz
+            out["source"] = self.source
+            out["scope"] = "warm-up, timed steps and the profiled pass of the headline workload"
+            out["timed_region"] = timed
+            return out
         rows = [r for r in csv.reader(io.StringIO(self.out or "")) if len(r) >= 9]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -127,7 +198,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": self.source}
 
 
 def make_V(workload, device, seed=20240501):
@@ -145,37 +216,160 @@ def make_V(workload, device, seed=20240501):
 _SAMPLES = {}
 
 
-def cpu_port_rate(workload, budget_s=12.0, max_rows=None):
-    """Oracle (plain OpenMP C restatement, FP32) iterations/s scaled to the full matrix."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    oracle.build()
+def host_V(workload, seed=20240501):
+    """The workload's V in host memory, generated as make_V does (on a GPU when
+    one is present, so that every arm sees the same matrix)."""
+    if workload in _SAMPLES:
+        return _SAMPLES[workload]
     _import_package()
     import nmf_b200.synth as synth
     n, m, k, gen, _ = WORKLOADS[workload]
-    rows = max_rows or max(500, min(n, int(1.5e7 // m)))  # ~15 M entries of the matrix
-    key = (workload, rows)
-    if key not in _SAMPLES:
+    V = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            V = make_V(workload, torch.device("cuda", 0), seed=seed).cpu().numpy()
+            torch.cuda.empty_cache()
+    except Exception:
+        V = None
+    if V is None:
         if gen == "poisson":
-            V, _ = synth.poisson_counts(rows, m, k, 7)
+            V, _ = synth.poisson_counts(n, m, k, seed)
         else:
-            V, _ = synth.expression_like(rows, m, k, 7, dirichlet=2.0, zero_frac=0.01)
-        _SAMPLES[key] = V
-    V = _SAMPLES[key]
-    W, H = oracle.init_random(3, rows, m, k)
-    t0 = time.perf_counter()
-    iters = 0
-    while True:
+            V, _ = synth.expression_like(n, m, k, seed, dirichlet=2.0, zero_frac=0.01)
+    _SAMPLES[workload] = V
+    return V
+
+
+def cpu_port_step(oracle, V, W, H, J):
+    """One step of the CPU restatement: J iterations of update_H + update_W,
+    the EPS adjust and the classification (the engine's step, on the CPU)."""
+    for _ in range(J):
         H = oracle.update_H(V, W, H)
         W = oracle.update_W(V, W, H)
-        iters += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or iters >= 200:
-            break
-    per_iter_full = el / iters * (n / rows)
-    return {"value": 1.0 / per_iter_full, "unit": "iters/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{iters} FP32 iterations of the oracle on a {rows}x{m} row sample ({el:.1f} s), "
-                      f"scaled by {n}/{rows} rows"}
+    H = oracle.adjust(H)
+    W = oracle.adjust(W)
+    oracle.classify(H)
+    return W, H
+
+
+def cpu_port_rate(workload, J=10, steps=1, warmup=0):
+    """Oracle (plain OpenMP C restatement, FP32, all host threads) iterations/s
+    on the workload's full matrix: `steps` timed steps of J iterations each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    n, m, k, gen, _ = WORKLOADS[workload]
+    V = host_V(workload)
+    W, H = oracle.init_random(3, n, m, k)
+    times = []
+    for s in range(warmup + steps):
+        t0 = time.perf_counter()
+        W, H = cpu_port_step(oracle, V, W, H, J)
+        if s >= warmup:
+            times.append(time.perf_counter() - t0)
+    el = sum(times)
+    return {"value": J * len(times) / el, "unit": "iters/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{J * len(times)} FP32 iterations ({len(times)} steps of {J} + adjust + classification) "
+                      f"of the oracle on the full {n}x{m} matrix, {el:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA build (oracle/_ref/NMF_GPU, compiled from the
+# reference sources by `make -C oracle ref`) timed on the same GPU.  It is a
+# baseline, never the measured product.
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "NMF_GPU")
+
+
+def _ref_input_path(tmp, name):
+    """The reference allocates strlen(filename) + strlen(ext) bytes for its
+    output name "<filename>_W<ext>" (src/NMF_GPU.c:974), three bytes short;
+    choose a path length whose malloc rounding leaves room for them."""
+    base = os.path.join(tmp, name)
+    while True:
+        s = len(base) + 4
+        chunk = max(32, (s + 8 + 15) & ~15)
+        if chunk - 8 >= s + 3:
+            return base
+        base += "_"
+
+
+def _write_nonnative(path, V):
+    """Non-native binary matrix file: u32 0xEDB10EA1, u32 rows, u32 cols, LE float64 data."""
+    import struct
+    n, m = V.shape
+    with open(path, "wb") as f:
+        f.write(struct.pack("<III", 0xEDB10EA1, n, m))
+        for r0 in range(0, n, 8192):
+            f.write(np.ascontiguousarray(V[r0:r0 + 8192], dtype="<f8").tobytes())
+
+
+def _ref_run(path, k, it, j, t, timeout=900):
+    """One NMF_GPU run; returns (seconds of its own TIME=1 line, iterations, converged)."""
+    import re
+    cmd = [REF_BIN, path, "-b", "0", "-e", "0", "-k", str(k), "-i", str(it), "-j", str(j), "-t", str(t)]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    out = p.stdout + p.stderr
+    if p.returncode != 0:
+        raise RuntimeError(f"NMF_GPU exited {p.returncode}: {out[-400:]}")
+    secs = float(re.search(r"GPU \+ classification \+ check_result time: ([0-9.eE+-]+)", out).group(1))
+    mc = re.search(r"converged in (\d+) iterations", out)
+    mp = re.search(r"NMF: (\d+) iterations performed", out)
+    return secs, int(mc.group(1) if mc else mp.group(1)), bool(mc)
+
+
+def reference_cuda_rates(pkg, dev, engine_rates, short=10, long=510):
+    """Iterations/s of the reference's CUDA build (cuBLAS SGEMMs + its own
+    kernels) on the same V and GPU: the difference of a `long`- and a
+    `short`-iteration run of its TIME=1 wall clock (which starts before the V
+    upload), so fixed costs cancel; plus its whole-run rate for `long`
+    iterations (V upload included, like the engine's e2e).  Config A runs to
+    convergence (-i 2000 -j 10 -t 40) and is compared on time to converge
+    with a whole solve through the engine's C ABI."""
+    import tempfile
+    if not os.path.exists(REF_BIN):
+        return {"unavailable": "oracle/_ref/NMF_GPU not built (make -C oracle ref needs the reference sources)"}
+    out = {"binary": "oracle/_ref/NMF_GPU (reference sources, single precision, cuBLAS, CPU_RANDOM init)",
+           "method": f"iters/s = {long - short} / (t(-i {long}) - t(-i {short})), t = its own TIME=1 line; "
+                     f"-j 10 -t 1e9 keeps the adjust cadence"}
+    with tempfile.TemporaryDirectory(dir="/tmp") as tmp:
+        for wl in ("C32", "B16"):
+            n, m, k, _, desc = WORKLOADS[wl]
+            path = _ref_input_path(tmp, wl)
+            _write_nonnative(path, host_V(wl))
+            t_s, _, _ = _ref_run(path, k, short, 10, 10 ** 9)
+            t_l, it_l, _ = _ref_run(path, k, long, 10, 10 ** 9)
+            rate = (long - short) / (t_l - t_s)
+            r = {"workload": desc, "value": rate, "unit": "iters/s", "run_seconds": {str(short): t_s, str(long): t_l},
+                 "e2e": {"value": it_l / t_l, "unit": "iters/s"},
+                 "roofline_frac_2nm4": 2.0 * n * m * 4 * rate / 1e9 / measured_peaks()[0]}
+            if wl in engine_rates:
+                r["engine_iters_per_s"] = engine_rates[wl]
+                r["engine_speedup"] = engine_rates[wl] / rate
+            out[wl] = r
+            os.unlink(path)
+        # config A: time to converge
+        import nmf_b200.synth as synth
+        Va, _ = synth.config_a(1)
+        path = _ref_input_path(tmp, "A")
+        _write_nonnative(path, Va)
+        ref = [_ref_run(path, 3, 2000, 10, 40) for _ in range(3)]
+        t_ref = min(r[0] for r in ref)
+        eng = []
+        for _ in range(4):
+            with pkg.NMF(Va.shape[0], Va.shape[1], 3, device=dev.index or 0) as e:
+                t0 = time.perf_counter()
+                e.set_V(Va)
+                e.init_random(3)
+                it, conv = e.run(2000, 10, 40)
+                e.distance()
+                eng.append((time.perf_counter() - t0, it, conv))
+        t_eng = min(x[0] for x in eng[1:])
+        out["A"] = {"workload": "5000x38 k=3 planted, -i 2000 -j 10 -t 40 (time to converge, V upload included)",
+                    "reference_seconds": t_ref, "reference_iterations": ref[0][1], "reference_converged": ref[0][2],
+                    "engine_seconds": t_eng, "engine_iterations": eng[-1][1], "engine_converged": eng[-1][2],
+                    "engine_speedup": t_ref / t_eng}
+    return out
 
 
 class L2Flush:
@@ -426,14 +620,10 @@ def run_reference_arm(a, rank, world):
     if rank != 0:
         return
     n, m, k, _, desc = WORKLOADS[a.workload]
-    rates = []
-    per_step = min(a.cpu_budget, 150.0 / max(1, a.steps + a.warmup))
-    for s in range(a.warmup + a.steps):
-        r = cpu_port_rate(a.workload, budget_s=per_step)
-        if s >= a.warmup:
-            rates.append(r["value"])
-    v = statistics.median(rates)
-    r["value"] = v
+    # every step is the engine's step (J iterations + adjust + classification)
+    # on the same full matrix; nothing is sampled or scaled
+    r = cpu_port_rate(a.workload, J=a.iters_per_step, steps=a.steps, warmup=a.warmup)
+    v = r["value"]
     line = {"impl": "reference", "metric": "KL-NMF iterations/s", "value": v, "unit": "iters/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * a.iters_per_step / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -472,6 +662,7 @@ def run_engine_arm(a, rank, world, local_rank):
     e.init_random(3)
     J = a.iters_per_step
     never = 2 ** 31
+    clk = ClockSampler(local_rank).__enter__()
     for _ in range(a.warmup):
         e.run(J, J, never)
     e.synchronize()
@@ -482,12 +673,13 @@ def run_engine_arm(a, rank, world, local_rank):
     torch.cuda.synchronize()
     l0 = e.launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        ev0.record(stream)
-        for _ in range(a.steps):
-            e.run(J, J, never)
-        ev1.record(stream)
-        ev1.synchronize()
+    clk.mark(True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        e.run(J, J, never)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk.mark(False)
     ms = ev0.elapsed_time(ev1)
     launches = e.launch_count() - l0
     # kernel times for the roofline: a separate pass with per-launch CUDA events
@@ -499,6 +691,7 @@ def run_engine_arm(a, rank, world, local_rank):
     e.synchronize()
     prof = {c: e.profile_read(c) for c in range(4)}
     e.profile(False)
+    clk.__exit__(None, None, None)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -546,7 +739,8 @@ def run_engine_arm(a, rank, world, local_rank):
                "d2h_bytes_per_step": (n + m) * kp * 4, "iters_per_step": E, "ms_per_step": e2e_ms}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cpu = cpu_port_rate(a.workload, budget_s=a.cpu_budget)
+        _SAMPLES[a.workload] = V.cpu().numpy()
+        cpu = cpu_port_rate(a.workload, J=a.iters_per_step, steps=1)
     e.close()
     extras = {}
     if rank == 0 and world == 1 and not a.no_extras:
@@ -563,6 +757,11 @@ def run_engine_arm(a, rank, world, local_rank):
                           for arm in ("bf16x3", "split_bf16", "bf16", "fused_tf32")}
         del V
         torch.cuda.empty_cache()
+        extras["workloads"] = {wl: guarded(workload_rate, a, pkg, dev, wl, hbm) for wl in ("C64", "B16")}
+        eng = {"C32": value}
+        if isinstance(extras["workloads"].get("B16"), dict) and "value" in extras["workloads"]["B16"]:
+            eng["B16"] = extras["workloads"]["B16"]["value"]
+        extras["reference_cuda"] = guarded(reference_cuda_rates, pkg, dev, eng)
         extras["sweep"] = guarded(sweep_rates, dev)
         extras["streamed"] = guarded(stream_rates, dev)
         extras["serving"] = guarded(serve_rates, dev)
@@ -578,6 +777,54 @@ def run_engine_arm(a, rank, world, local_rank):
             "clocks": clk.summary()}
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def workload_rate(a, pkg, dev, wl, hbm, steps=20, arm="fused"):
+    """The fused arm on another workload: iterations/s (steps of J iterations,
+    L2 flushed before every timed step: B16's V fits in L2) and the dominant
+    kernel's HBM fraction."""
+    import torch
+    n, m, k, _, desc = WORKLOADS[wl]
+    V = make_V(wl, dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = L2Flush(dev)
+    e = pkg.NMF(n, m, k, arm=arm, device=dev.index or 0)
+    try:
+        e.set_stream(stream.cuda_stream)
+        e.set_V_device(V.data_ptr(), m)
+        e.init_random(3)
+        J = a.iters_per_step
+        for _ in range(3):
+            e.run(J, J, 2 ** 31)
+        e.synchronize()
+        ms = 0.0
+        for _ in range(steps):
+            flush(stream)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            e.run(J, J, 2 ** 31)
+            ev1.record(stream)
+            ev1.synchronize()
+            ms += ev0.elapsed_time(ev1)
+        e.profile(True)
+        e.run(J, J, 2 ** 31)
+        e.synchronize()
+        prof = {c: e.profile_read(c) for c in range(4)}
+        e.profile(False)
+    finally:
+        e.close()
+        del V, flush
+        torch.cuda.empty_cache()
+    cls = 0 if prof[0][0] >= prof[1][0] else 1
+    kms = prof[cls][0] / max(prof[cls][1], 1)
+    value = steps * J / (ms / 1e3)
+    return {"workload": desc, "value": value, "unit": "iters/s", "steps": steps, "iters_per_step": J,
+            "l2": "256 MB written before every timed step" + (" (V fits in L2: within a step it is re-read from L2)"
+                                                              if n * m * 4 < 126e6 else ""),
+            "roofline": {"kernel": ("update_H" if cls == 0 else "update_W") + f"[{arm}]", "avg_launch_ms": kms,
+                         "achieved": n * m * 4 / (kms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": n * m * 4 / (kms / 1e3) / 1e9 / hbm},
+            "iteration_frac_2nm4": 2.0 * n * m * 4 * value / 1e9 / hbm}
 
 
 def other_arm_rate(a, pkg, V, dev, stream, n, m, k, hbm, arm, steps=5):
@@ -652,7 +899,6 @@ def main():
     ap.add_argument("--workload", default="C32", choices=list(WORKLOADS))
     ap.add_argument("--iters-per-step", type=int, default=10)
     ap.add_argument("--e2e-iters", type=int, default=500)
-    ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-arm and sweep measurements")

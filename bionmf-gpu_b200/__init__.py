@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_profile_read": ([vp, i32, C.POINTER(C.c_double), C.POINTER(u32)], i32),
         "nmfb_synchronize": ([vp], i32),
         "nmfb_launch_count": ([vp], C.c_uint64),
+        "nmfb_set_wait_limit": ([vp, C.c_uint64], i32),
         "nmfb_update_H_noalloc": ([vp, sz, vp, sz, vp, sz, u32, u32, u32, vp], i32),
         "nmfb_batch_create": ([C.POINTER(vp), i32, u32, u32, u32, C.POINTER(u32)], i32),
         "nmfb_batch_destroy": ([vp], i32),
@@ -317,6 +318,10 @@ class NMF:
 
     def launch_count(self) -> int:
         return int(self._L.nmfb_launch_count(self._h))
+
+    def set_wait_limit(self, ns: int):
+        """Limit of the fused kernels' bounded device waits in ns (0: default, 1 s)."""
+        self._check(self._L.nmfb_set_wait_limit(self._h, int(ns)))
 
 
 def _uptr(a: np.ndarray):

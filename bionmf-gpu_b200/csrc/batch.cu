@@ -510,6 +510,19 @@ __device__ void run_problem(Problem &P, float *sm, uint32_t *s_ctl, const Slice 
                 s_ctl[1] = 1;
         }
         __syncthreads();
+        if (X.size > 1) {
+            // Every CTA of the cluster holds the same H and labels, so their stop
+            // decisions agree; still, take rank 0's, so that the cluster barriers
+            // of the next iteration are reached by all CTAs or by none.  The
+            // second barrier keeps rank 0 from changing s_ctl before the others
+            // have read it.
+            cg::cluster_group const cl = cg::this_cluster();
+            cl.sync();
+            uint32_t const stop0 = *cl.map_shared_rank(&s_ctl[1], 0u);
+            cl.sync();
+            if (tid == 0) s_ctl[1] = stop0;
+            __syncthreads();
+        }
         if (s_ctl[1]) break;
     }
     if (!s_ctl[1])
@@ -1552,13 +1565,15 @@ int nmfb_serve_poll(nmfb_serve *s, uint32_t ticket, int *done)
 {
     if (!s || !done) return NMFB_EINVAL;
     uint32_t const slot = ticket % s->capacity;
+    // The slot is rewritten by submit and fetch under the lock; read it under
+    // the lock too, so a poll from one host thread never races them.
+    std::lock_guard<std::mutex> lock(s->mu);
     if (s->slots[slot].ticket != ticket + 1u) return sfail(s, NMFB_EINVAL, "ticket %u is not pending", ticket);
     *done = (s->hDone[4 * (size_t)slot] == ticket + 1u) ? 1 : 0;
     if (*done) {
         std::atomic_thread_fence(std::memory_order_acquire);
         return NMFB_OK;
     }
-    std::lock_guard<std::mutex> lock(s->mu);
     STRY(s, cudaSetDevice(s->device));
     return serve_ensure_running(s);
 }

@@ -81,20 +81,36 @@ __device__ __forceinline__ uint64_t policy_evict_last()
     return p;
 }
 
-// Bounded wait: false on timeout or when another role already aborted.
+// Bounded wait: false once `limit_ns` of %globaltimer pass (the wait then sets
+// the CTA's abort flag and records `code` in the error word) or when another
+// role already aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort_flag,
-                                          uint32_t *err, uint32_t code)
+                                          uint32_t *err, uint32_t code, unsigned long long limit_ns)
 {
     if (mbar_try_wait(bar, parity)) return true;
     unsigned long long const t0 = globaltimer();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort_flag) return false;
-        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+        if (globaltimer() - t0 > limit_ns) {
             *abort_flag = 1;
             atomicExch(err, code);
             return false;
         }
     }
+    return true;
+}
+
+// Drain wait, used after a role has stopped (normally or on abort): waits for
+// a phase of asynchronous work this thread issued itself (a TMA load's
+// complete_tx, an MMA commit) to land, ignoring the abort flag, for at most
+// WAIT_LIMIT_NS.  Nothing of the CTA may still be written by the async proxy
+// when it frees its tensor memory and exits.
+__device__ __forceinline__ bool mbar_drain(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    unsigned long long const t0 = globaltimer();
+    while (!mbar_try_wait(bar, parity))
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) return false;
     return true;
 }
 
@@ -115,6 +131,15 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+
+// Drain of every tcgen05.mma the calling thread has issued: one more commit
+// (it arrives once all earlier MMAs of this thread have completed) on a
+// barrier used for nothing else, then a drain wait on it.
+__device__ __forceinline__ void mma_drain(uint64_t *bar)
+{
+    tc_commit(bar);
+    mbar_drain(bar, 0);
 }
 
 __device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc, uint32_t acc)

@@ -117,6 +117,7 @@ struct ArgsB {
     float *part;
     uint32_t *err;
     const ConvState *st;
+    unsigned long long wait_ns;  // limit of every bounded wait (%globaltimer ns)
 };
 
 // BF16 hi / lo copies of a factor (rows x kp FP32, padding columns zero) and,
@@ -183,7 +184,8 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
     uint64_t *const accrdy = rempty + G::NRB;        // [2]    MMA2 commit -> accumulator warps
     uint64_t *const accfree = accrdy + 2;            // [2]    accumulator warps -> MMA2
     uint64_t *const xfull = accfree + 2;             // [1]    TMA -> MMA1
-    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xfull + 1);
+    uint64_t *const mdrain = xfull + 1;              // [1]    issuer's final commit (drain)
+    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(mdrain + 1);
     volatile uint32_t *const abort_flag = tmem_slot + 1;
 
     uint32_t const warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -214,6 +216,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
             mbar_init(&accfree[b], 4);
         }
         mbar_init(xfull, 1);
+        mbar_init(mdrain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -234,11 +237,13 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
         // ------------------------------------------------------------ V producer
         if (lane == 0) {
             uint64_t const pol = policy_evict_first();
+            uint32_t issued = 0;
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::VST;
                 if (t >= (uint32_t)G::VST &&
-                    !mbar_wait(&vempty[s], ((t / G::VST) - 1) & 1, abort_flag, args.err, 21u))
+                    !mbar_wait(&vempty[s], ((t / G::VST) - 1) & 1, abort_flag, args.err, 21u, args.wait_ns))
                     break;
+                issued = t + 1;
                 unsigned char *sv = sV + s * G::VBYTES;
                 int const r0 = (int)((t_begin + t) * BR);
                 mbar_expect_tx(&vfull[s], G::VBYTES);
@@ -250,6 +255,9 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                         tma_load_2d(sv + b * (BO * 128), &maps.v, &vfull[s], r0 + 32 * b, (int)o0, pol);
                 }
             }
+            // drain: the last load into every stage has landed
+            for (uint32_t t = issued > (uint32_t)G::VST ? issued - G::VST : 0; t < issued; t++)
+                mbar_drain(&vfull[t % G::VST], (t / G::VST) & 1);
         }
     } else if (warp == 2) {
         // ------------------------------------------------------------ X and Y producer
@@ -258,11 +266,13 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
             mbar_expect_tx(xfull, (SPLIT ? 2 : 1) * G::XBYTES);
             tma_load_2d(sX, &maps.xh, xfull, 0, (int)o0, pol);
             if (SPLIT) tma_load_2d(sX + G::XBYTES, &maps.xl, xfull, 0, (int)o0, pol);
+            uint32_t issued = 0;
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::YST;
                 if (t >= (uint32_t)G::YST &&
-                    !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 22u))
+                    !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 22u, args.wait_ns))
                     break;
+                issued = t + 1;
                 unsigned char *sy = sY + s * G::YSTAGE;
                 int const r0 = (int)((t_begin + t) * BR);
                 mbar_expect_tx(&yfull[s], (SPLIT ? 2 : 1) * G::YBYTES + G::YTROWS * 128);
@@ -270,6 +280,10 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                 if (SPLIT) tma_load_2d(sy + G::YBYTES, &maps.yl, &yfull[s], 0, r0, pol);
                 tma_load_2d(sy + 2 * G::YBYTES, &maps.yt, &yfull[s], 0, (int)((t_begin + t) * 2 * KP), pol);
             }
+            // drain: X and the last load into every Y stage have landed
+            mbar_drain(xfull, 0);
+            for (uint32_t t = issued > (uint32_t)G::YST ? issued - G::YST : 0; t < issued; t++)
+                mbar_drain(&yfull[t % G::YST], (t / G::YST) & 1);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -286,7 +300,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
             uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dYT0 = smem_desc(smem_u32(sY + 2 * G::YBYTES), 16, 1024, 2u);
             uint64_t const dR0 = smem_desc(smem_u32(sR), 16, 1024, 2u);
-            bool ok = mbar_wait(xfull, 0, abort_flag, args.err, 23u);
+            bool ok = mbar_wait(xfull, 0, abort_flag, args.err, 23u, args.wait_ns);
             tc_fence_after();
             uint32_t n1 = 0, n2 = 0;
             unsigned long long last = globaltimer();
@@ -339,7 +353,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                     last = globaltimer();
                 } else if (*abort_flag) {
                     ok = false;
-                } else if (globaltimer() - last > WAIT_LIMIT_NS) {
+                } else if (globaltimer() - last > args.wait_ns) {
                     *abort_flag = 1;
                     atomicExch(args.err, 24u);
                     ok = false;
@@ -347,6 +361,9 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                     __nanosleep(64);
                 }
             }
+            // drain: every MMA issued above has completed before the CTA frees
+            // the shared and tensor memory it reads and writes
+            mma_drain(mdrain);
         }
     } else if (warp >= 4 && warp < 4 + NR) {
         // ------------------------------------------------------------ R warps
@@ -356,9 +373,10 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
         for (uint32_t t = 0; t < T; t++) {
             uint32_t const s = t % G::VST, b = t % G::NDB, rs = t % G::NRB;
-            if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 25u)) break;
-            if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 26u)) break;
-            if (t >= (uint32_t)G::NRB && !mbar_wait(&rempty[rs], ((t / G::NRB) - 1) & 1, abort_flag, args.err, 27u))
+            if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 25u, args.wait_ns)) break;
+            if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 26u, args.wait_ns)) break;
+            if (t >= (uint32_t)G::NRB &&
+                !mbar_wait(&rempty[rs], ((t / G::NRB) - 1) & 1, abort_flag, args.err, 27u, args.wait_ns))
                 break;
             tc_fence_after();
             const unsigned char *sv = sV + s * G::VBYTES;
@@ -425,7 +443,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
         bool ok = true;
         for (uint32_t t = 0; ok && t < T; t++) {
             uint32_t const bp = t & 1;
-            if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 28u)) {
+            if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 28u, args.wait_ns)) {
                 ok = false;
                 break;
             }
@@ -558,6 +576,7 @@ int launch_b(nmfb_ctx *ctx, const MapsB &maps, uint32_t *err)
     args.part = ctx->dPart;
     args.err = err;
     args.st = ctx->dState;
+    args.wait_ns = ctx->wait_ns ? ctx->wait_ns : WAIT_LIMIT_NS;
     int const main = HSIDE ? 0 : 1;
     int rc = nmfb_prof_begin(ctx, main);
     if (rc) return rc;

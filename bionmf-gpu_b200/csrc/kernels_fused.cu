@@ -66,6 +66,7 @@ struct FusedArgs {
     uint32_t *err;        // device error word
     const ConvState *st;
     const float *X;       // factor being updated (O x KP), read once per CTA into TMEM
+    unsigned long long wait_ns;  // limit of every bounded wait (%globaltimer ns)
 #ifdef NMFB_FUSED_DEBUG
     float *dbg;           // block 0, tile 0: D | V | Rh | Acc (debug builds only; 128 x 64 each)
 #endif
@@ -172,7 +173,8 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     uint64_t *const accrdy = rfull + G::NDB;        // [2]    MMA2 commit -> accumulator warps
     uint64_t *const accfree = accrdy + 2;           // [2]    accumulator warps -> MMA2
     uint64_t *const xready = accfree + 2;           // [1]    X split into TMEM -> MMA1
-    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(xready + 1);
+    uint64_t *const mdrain = xready + 1;            // [1]    issuer's final commit (drain)
+    uint32_t *const tmem_slot = reinterpret_cast<uint32_t *>(mdrain + 1);
     volatile uint32_t *const abort_flag = tmem_slot + 1;
 
     uint32_t const warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -219,6 +221,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             mbar_init(&accfree[b], 4);
         }
         mbar_init(xready, 4);
+        mbar_init(mdrain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -239,11 +242,13 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         // ------------------------------------------------------------ V producer
         if (lane == 0) {
             uint64_t const pol = policy_evict_first();
+            uint32_t issued = 0;
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::VST;
                 if (t >= (uint32_t)G::VST &&
-                    !mbar_wait(&vempty[s], ((t / G::VST) - 1) & 1, abort_flag, args.err, 1u))
+                    !mbar_wait(&vempty[s], ((t / G::VST) - 1) & 1, abort_flag, args.err, 1u, args.wait_ns))
                     break;
+                issued = t + 1;
                 unsigned char *sv = sV + s * G::VBYTES;
                 int const r0 = (int)((t_begin + t) * BR);
                 DBG_TS(0, t);
@@ -256,16 +261,22 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                         tma_load_2d(sv + b * (BO * 128), &maps.v, &vfull[s], r0 + 32 * b, (int)o0, pol);
                 }
             }
+            // drain: the last load into every stage has landed (each earlier one
+            // had to, before its stage was released for reuse)
+            for (uint32_t t = issued > (uint32_t)G::VST ? issued - G::VST : 0; t < issued; t++)
+                mbar_drain(&vfull[t % G::VST], (t / G::VST) & 1);
         }
     } else if (warp == 2) {
         // ------------------------------------------------------------ Y producer
         if (lane == 0) {
             uint64_t const pol = policy_evict_last();
+            uint32_t issued = 0;
             for (uint32_t t = 0; t < T; t++) {
                 uint32_t const s = t % G::YST;
                 if (t >= (uint32_t)G::YST &&
-                    !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 2u))
+                    !mbar_wait(&yempty[s], ((t / G::YST) - 1) & 1, abort_flag, args.err, 2u, args.wait_ns))
                     break;
+                issued = t + 1;
                 unsigned char *syh = sY + s * G::YSTAGE;
                 int const r0 = (int)((t_begin + t) * BR);
                 DBG_TS(1, t);
@@ -277,6 +288,8 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                 // Y^T: the BR / 32 row blocks of this tile, 2 KP rows of 128 B each
                 tma_load_2d(sYT + s * G::YTSTAGE, &maps.yt, &yfull[s], 0, (r0 / 32) * 2 * KP, pol);
             }
+            for (uint32_t t = issued > (uint32_t)G::YST ? issued - G::YST : 0; t < issued; t++)
+                mbar_drain(&yfull[t % G::YST], (t / G::YST) & 1);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -295,7 +308,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             // every operand lies below 256 KB).
             uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dYT0 = smem_desc(smem_u32(sYT), 16, 1024, 2u);
-            bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u);
+            bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u, args.wait_ns);
             tc_fence_after();
             uint32_t n1 = 0, n2 = 0;
             unsigned long long last = globaltimer();
@@ -358,7 +371,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                     last = globaltimer();
                 } else if (*abort_flag) {
                     ok = false;
-                } else if (globaltimer() - last > WAIT_LIMIT_NS) {
+                } else if (globaltimer() - last > args.wait_ns) {
                     *abort_flag = 1;
                     atomicExch(args.err, 4u);
                     ok = false;
@@ -366,6 +379,9 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                     __nanosleep(0);
                 }
             }
+            // drain: every MMA issued above has completed (and with it its reads of
+            // shared memory and writes of tensor memory) before the CTA frees them
+            mma_drain(mdrain);
         }
     } else if (warp >= 4 && warp < 4 + NR) {
         // ------------------------------------------------------------ R warps
@@ -377,9 +393,9 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             uint32_t const s = t % G::VST, b = t % G::NDB;
             if (warp == 4 && lane == 0) DBG_TS(4, t);
             DBG_PH(0, t);
-            if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 6u)) break;
+            if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 6u, args.wait_ns)) break;
             DBG_PH(1, t);
-            if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u)) break;
+            if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 7u, args.wait_ns)) break;
             tc_fence_after();
             DBG_PH(2, t);
             if (warp == 4 && lane == 0) DBG_TS(5, t);
@@ -500,7 +516,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         }
         for (uint32_t t = 0; ok && t < T; t++) {
             uint32_t const bp = t & 1;
-            if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 8u)) { ok = false; break; }
+            if (!mbar_wait(&accrdy[bp], (t >> 1) & 1, abort_flag, args.err, 8u, args.wait_ns)) { ok = false; break; }
             tc_fence_after();
             // Acc columns [0, KP) and, for the 3-term arm, [KP, 2 KP) both add to sum.
 #pragma unroll
@@ -632,6 +648,7 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
     args.err = plan->dErr;
     args.st = ctx->dState;
     args.X = HSIDE ? ctx->dH : ctx->dW;
+    args.wait_ns = ctx->wait_ns ? ctx->wait_ns : WAIT_LIMIT_NS;
 #ifdef NMFB_FUSED_DEBUG
     args.dbg = plan->dDbg;
 #endif
@@ -767,6 +784,9 @@ uint32_t *nmfb_fused_err_word(nmfb_ctx *ctx)
     return plan ? plan->dErr : nullptr;
 }
 
+// Reads the fused kernels' error word (the site of the first bounded wait that
+// ran out, 0 if none) and clears it, so each expiry is reported once and the
+// context stays usable.
 int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
 {
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
@@ -774,6 +794,10 @@ int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
     if (!plan) return NMFB_OK;
     NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(code, plan->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (*code) {
+        NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
+        NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     return NMFB_OK;
 }
 

@@ -488,7 +488,8 @@ static int launch_block(nmfb_ctx *ctx, uint32_t J)
 {
     static int const use_graphs = getenv("NMFB_NO_GRAPHS") == nullptr;
     if (!use_graphs || ctx->prof_on || ctx->splan) return enqueue_block(ctx, J);
-    if (!ctx->blk_exec || ctx->blk_J != J || ctx->blk_arm != ctx->arm || ctx->blk_stream != ctx->stream) {
+    if (!ctx->blk_exec || ctx->blk_J != J || ctx->blk_arm != ctx->arm || ctx->blk_stream != ctx->stream ||
+        ctx->blk_wait != ctx->wait_ns) {
         if (ctx->blk_exec) {
             NMFB_CUDA_TRY(ctx, cudaGraphExecDestroy(ctx->blk_exec));
             ctx->blk_exec = nullptr;
@@ -513,6 +514,7 @@ static int launch_block(nmfb_ctx *ctx, uint32_t J)
         ctx->blk_J = J;
         ctx->blk_arm = ctx->arm;
         ctx->blk_stream = ctx->stream;
+        ctx->blk_wait = ctx->wait_ns;
     }
     NMFB_CUDA_TRY(ctx, cudaGraphLaunch(ctx->blk_exec, ctx->stream));
     ctx->launches += ctx->blk_kernels;
@@ -730,5 +732,13 @@ int nmfb_synchronize(nmfb_ctx *ctx)
 }
 
 uint64_t nmfb_launch_count(const nmfb_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int nmfb_set_wait_limit(nmfb_ctx *ctx, uint64_t ns)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    ctx->wait_ns = (unsigned long long)ns;
+    return NMFB_OK;
+}
 
 }  // extern "C"

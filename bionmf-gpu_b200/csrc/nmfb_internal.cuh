@@ -57,6 +57,7 @@ struct nmfb_ctx {
     nmfb::ConvState *hState;  // pinned host mirror
 
     uint64_t launches;
+    unsigned long long wait_ns;  // bounded-wait limit of the fused kernels (0: the 1 s default)
     // CUDA graph of one convergence-test block (nmfb_run): replayed instead of
     // re-launching its ~12 kernels per iteration; rebuilt when J, the arm or
     // the stream change.
@@ -64,6 +65,7 @@ struct nmfb_ctx {
     uint32_t blk_J;
     int blk_arm;
     cudaStream_t blk_stream;
+    unsigned long long blk_wait;
     uint64_t blk_kernels;
     cudaStream_t own_stream;
 

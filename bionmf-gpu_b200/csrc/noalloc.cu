@@ -24,8 +24,10 @@
 // different host threads) race on it and both results are undefined.
 //
 // Host code sees g_noalloc_scratch only as a host-side stand-in symbol; the
-// device address comes from cudaGetSymbolAddress, taken once per device on the
-// first call made while that device is current and cached afterwards.
+// device address comes from cudaGetSymbolAddress, taken on the first call made
+// while a device is current and cached with that device's current context (a
+// call under a different context -- after cudaDeviceReset, say -- takes it
+// again).  Make the first call on a device before any stream capture.
 //
 // The arithmetic follows the reference's update_H (src/NMF_routines.c:704-1000
 // with kernel_mul_div, src/GPU_kernels.cu:1886-2058): colsum(W) in FP64 summed in split order,
@@ -134,20 +136,44 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_finish(float *__restrict__ H,
 
 struct DeviceSlot {
     bool ready;
-    unsigned char *scratch;   // device address of g_noalloc_scratch on this device
+    void *cu_ctx;             // CUDA context the address below belongs to
+    unsigned char *scratch;   // device address of g_noalloc_scratch in that context
     int sm_count;
 };
 
 std::mutex g_slot_mutex;
 DeviceSlot g_slots[NA_MAX_DEV];
 
-// Once per device, with that device current: resolve the scratch array's
-// device address and the SM count.  Allocates nothing.
+// The calling thread's current CUDA context (driver cuCtxGetCurrent, found
+// through the runtime's entry-point query so the library links only cudart).
+void *current_cu_ctx()
+{
+    typedef int (*GetCurrent)(void **);
+    static GetCurrent fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<GetCurrent>(p);
+    }
+    void *c = nullptr;
+    if (!fn || fn(&c) != 0) return nullptr;
+    return c;
+}
+
+// With the device current: resolve the scratch array's device address and the
+// SM count, once per device and context.  The address is cached with the
+// context it was taken in: after cudaDeviceReset, or under another context of
+// the same device, the module is loaded anew at another address, so a changed
+// context resolves it again.  Allocates nothing.
 int device_slot(int dev, DeviceSlot *out)
 {
     std::lock_guard<std::mutex> lock(g_slot_mutex);
     DeviceSlot &slot = g_slots[dev];
-    if (!slot.ready) {
+    void *const cu_ctx = current_cu_ctx();
+    if (!slot.ready || slot.cu_ctx != cu_ctx) {
+        slot.ready = false;
         int major = 0, sms = 0;
         if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
@@ -162,6 +188,7 @@ int device_slot(int dev, DeviceSlot *out)
         }
         slot.scratch = static_cast<unsigned char *>(ptr);
         slot.sm_count = sms;
+        slot.cu_ctx = cu_ctx;
         slot.ready = true;
     }
     *out = slot;

@@ -189,6 +189,15 @@ int nmfb_synchronize(nmfb_ctx *ctx);
 /* Kernel launches issued by this context since creation (for accounting). */
 uint64_t nmfb_launch_count(const nmfb_ctx *ctx);
 
+/* Limit, in nanoseconds, of every bounded device-side wait of the fused
+ * kernels (0 restores the default, 1 s).  A wait that runs out makes its CTA
+ * stop, drain the copies and tensor-core work it has in flight and exit; the
+ * next nmfb_run / nmfb_synchronize returns NMFB_ETIMEOUT once (the factors are
+ * then undefined; the context stays usable after nmfb_init_random or
+ * nmfb_set_WH).  No counterpart in the reference, whose kernels do not wait
+ * on one another. */
+int nmfb_set_wait_limit(nmfb_ctx *ctx, uint64_t ns);
+
 /* ---------------------------------------------------------------------------
  * Batched solves: rank-selection and restart sweeps.  The reference runs one
  * factorisation per process (nmf(), src/NMF_GPU.c:522-795; its user guide,

@@ -81,3 +81,18 @@ def maxnorm_rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def assert_labels_match(labels, H_ref, classify, margin=1e-3, min_checked=0.99):
+    """Classification parity against a reference H: bit-exact on every sample
+    whose two largest entries in H_ref differ by more than `margin` (relative);
+    samples closer than that are ties at the factors' own tolerance and are
+    not compared.  At least `min_checked` of the samples must be compared."""
+    H_ref = np.asarray(H_ref, np.float64)
+    srt = np.sort(H_ref, axis=1)
+    top, second = srt[:, -1], srt[:, -2] if H_ref.shape[1] > 1 else np.zeros(H_ref.shape[0])
+    sep = (top - second) > margin * np.abs(top)
+    assert sep.mean() >= min_checked, f"only {sep.mean():.3f} of the samples are separated"
+    ref = classify(H_ref)
+    bad = np.nonzero((np.asarray(labels) != ref) & sep)[0]
+    assert bad.size == 0, f"{bad.size} separated samples classified differently, e.g. {bad[:5]}"

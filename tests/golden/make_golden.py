@@ -6,7 +6,7 @@ its parity mode: CPU_RANDOM (glibc srandom/random initialisation) and
 FIXED_INIT (seed 3) -- on seeded synthetic inputs, reading back its binary
 outputs (``-e 0``: little-endian float64) and its stdout.  Needs a GPU.
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <directory> [--cases NAME ...]
 
 Each case is written as ``<case>.npz`` holding the input V (float32; for
 inputs above 200k entries only the generator call and the SHA-256 of V), the
@@ -68,6 +68,10 @@ CASES = {
     "r400x128_k100": (("expression_like", dict(n=400, m=128, k=100, seed=14)), 100, 10, 5, 100),
     "B_small_k16": (("expression_like", dict(n=2000, m=300, k=16, seed=15, dirichlet=2.0, zero_frac=0.01)),
                     16, 100, 10, 1000000),
+    # the benchmarked config B matrix (20000 x 1000, k = 16, 1 % zeros) and the
+    # 6000 x 500 submatrix of the precision comparison, fixed iteration counts
+    "B_k16_fixed100": (("config_b", {}), 16, 100, 10, 1000000),
+    "Csub_6000x500_k32": (("poisson_counts", dict(n=6000, m=500, k=32, seed=63)), 32, 50, 10, 1000000),
 }
 
 
@@ -121,7 +125,7 @@ def run_case(name, spec, outdir, tmp):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory for the <case>.npz fixtures and summary.json")
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     a = ap.parse_args()
     if not os.path.exists(REF_BIN):

@@ -1,0 +1,111 @@
+"""GPU parity at the sizes the benchmark reports.
+
+The small-shape parity tests cover the update rules and the loop; these run
+the same comparisons on the geometries the measured numbers come from, so
+that every benchmarked configuration carries its own correctness check:
+
+  * 60000 x 5000, k = 32 and k = 64 (the headline workload): 469 / 40 output
+    row blocks, hundreds of reduction tiles split over several CTAs and summed
+    by the split epilogue -- a few iterations against the FP64 oracle;
+  * the 6000 x 500 C-submatrix at k = 32 and k = 64 with the fused (3xTF32)
+    and BF16x3 arms: W / H after a fixed count, KL, classification;
+  * config B, 20000 x 1000, k = 16, 1 % exact zeros.
+
+Tolerances (as in the small-shape tests): W, H within 1e-4 of the FP64 oracle
+(max|dX| / max|X|) after a fixed iteration count; the final KL divergence
+within 1e-5 relative of the FP64 oracle's; classification bit-exact on every
+sample whose top two factor loadings differ by more than 1e-3 (closer ones
+are ties at the factors' own tolerance; at least 99 % of samples qualify,
+90 % after the headline case's three iterations from the random start).  The
+BF16x3 arm is held to its stated bounds (W / H 1e-3, KL 1e-5).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import assert_labels_match, maxnorm_rel
+
+pytestmark = pytest.mark.gpu
+
+NEVER = 10 ** 9
+
+
+def _run(pkg, V, k, arm, n_iters, j=10, seed=3):
+    n, m = V.shape
+    with pkg.NMF(n, m, k, arm=arm) as e:
+        e.set_V(V)
+        e.init_random(seed)
+        it, conv = e.run(n_iters, j, NEVER)
+        assert (it, conv) == (n_iters, False)
+        return e.W, e.H, e.classification(), e.kl_divergence()
+
+
+def _poisson(synth, n, m, k, seed):
+    import torch
+    V, _ = synth.poisson_counts(n, m, k, seed, device=torch.device("cuda", 0))
+    out = V.cpu().numpy()
+    del V
+    torch.cuda.empty_cache()
+    return out
+
+
+@pytest.mark.parametrize("k", [32, 64])
+def test_headline_geometry_fixed_iterations(pkg, oracle, synth, k):
+    # The benchmarked matrix itself: every row block and reduction split of
+    # both halves.  Three iterations keep the FP64 oracle to seconds.
+    V = _poisson(synth, 60000, 5000, k, 20240501)
+    n, m = V.shape
+    iters = 3
+    W0, H0 = oracle.init_random(3, n, m, k)
+    W64, H64, _, _ = oracle.nmf(V, W0, H0, iters, 10, NEVER, prec="f64")
+    W, H, lab, _ = _run(pkg, V, k, "fused", iters)
+    assert maxnorm_rel(W, W64) < 1e-4
+    assert maxnorm_rel(H, H64) < 1e-4
+    # three iterations from a random start leave a few percent of the samples
+    # with near-tied loadings; the separated ones must agree exactly
+    assert_labels_match(lab, H64, oracle.classify, min_checked=0.9)
+
+
+_SUB = {}
+
+
+def _c_submatrix_oracle(oracle, synth, k):
+    """V, and the FP64 oracle's factors after 20 and 200 iterations (cached per k)."""
+    if k not in _SUB:
+        V, _ = synth.poisson_counts(6000, 500, k, 31 + k)
+        n, m = V.shape
+        W0, H0 = oracle.init_random(3, n, m, k)
+        W20, H20, _, _ = oracle.nmf(V, W0, H0, 20, 10, NEVER, prec="f64")
+        W200, H200, _, _ = oracle.nmf(V, W0, H0, 200, 10, NEVER, prec="f64")
+        kl200 = oracle.kl_divergence(V, W200.astype(np.float32), H200.astype(np.float32))
+        _SUB[k] = (V, W20, H20, kl200)
+    return _SUB[k]
+
+
+@pytest.mark.parametrize("arm,wtol", [("fused", 1e-4), ("bf16x3", 1e-3)])
+@pytest.mark.parametrize("k", [32, 64])
+def test_c_submatrix(pkg, oracle, synth, arm, wtol, k):
+    V, W64, H64, kl64 = _c_submatrix_oracle(oracle, synth, k)
+    # fixed count: factors
+    W, H, lab, _ = _run(pkg, V, k, arm, 20)
+    assert maxnorm_rel(W, W64) < wtol
+    assert maxnorm_rel(H, H64) < wtol
+    assert_labels_match(lab, H64, oracle.classify)
+    # longer run: the divergence
+    _, _, _, kl = _run(pkg, V, k, arm, 200)
+    assert abs(kl - kl64) <= 1e-5 * abs(kl64)
+
+
+def test_config_b_fixed_iterations(pkg, oracle, synth):
+    V, _ = synth.config_b(2)
+    n, m = V.shape
+    assert (V == 0).mean() > 0.009
+    W0, H0 = oracle.init_random(3, n, m, 16)
+    W64, H64, _, _ = oracle.nmf(V, W0, H0, 30, 10, NEVER, prec="f64")
+    W, H, lab, kl = _run(pkg, V, 16, "fused", 30)
+    assert maxnorm_rel(W, W64) < 1e-4
+    assert maxnorm_rel(H, H64) < 1e-4
+    assert_labels_match(lab, H64, oracle.classify)
+    kl64 = oracle.kl_divergence(V, W64.astype(np.float32), H64.astype(np.float32))
+    assert abs(kl - kl64) <= 1e-5 * abs(kl64)
