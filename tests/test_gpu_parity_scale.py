@@ -13,7 +13,10 @@ that every benchmarked configuration carries its own correctness check:
 
 Tolerances (as in the small-shape tests): W, H within 1e-4 of the FP64 oracle
 (max|dX| / max|X|) after a fixed iteration count; the final KL divergence
-within 1e-5 relative of the FP64 oracle's; classification bit-exact on every
+within 1e-5 relative of the FP64 oracle's, taken after 1000 iterations, where
+the C-submatrix's divergence has settled (the FP32 oracle is then within 2e-7
+of FP64; after 200 iterations, while it still falls steeply, FP32 and FP64
+trajectories differ by up to 2e-4 in KL); classification bit-exact on every
 sample whose top two factor loadings differ by more than 1e-3 (closer ones
 are ties at the factors' own tolerance; at least 99 % of samples qualify,
 90 % after the headline case's three iterations from the random start).  The
@@ -68,18 +71,20 @@ def test_headline_geometry_fixed_iterations(pkg, oracle, synth, k):
 
 
 _SUB = {}
+KL_ITERS = 1000
 
 
 def _c_submatrix_oracle(oracle, synth, k):
-    """V, and the FP64 oracle's factors after 20 and 200 iterations (cached per k)."""
+    """V, the FP64 oracle's factors after 20 iterations and its divergence after
+    KL_ITERS (cached per k)."""
     if k not in _SUB:
         V, _ = synth.poisson_counts(6000, 500, k, 31 + k)
         n, m = V.shape
         W0, H0 = oracle.init_random(3, n, m, k)
         W20, H20, _, _ = oracle.nmf(V, W0, H0, 20, 10, NEVER, prec="f64")
-        W200, H200, _, _ = oracle.nmf(V, W0, H0, 200, 10, NEVER, prec="f64")
-        kl200 = oracle.kl_divergence(V, W200.astype(np.float32), H200.astype(np.float32))
-        _SUB[k] = (V, W20, H20, kl200)
+        Wf, Hf, _, _ = oracle.nmf(V, W0, H0, KL_ITERS, 10, NEVER, prec="f64")
+        klf = oracle.kl_divergence(V, Wf.astype(np.float32), Hf.astype(np.float32))
+        _SUB[k] = (V, W20, H20, klf)
     return _SUB[k]
 
 
@@ -92,8 +97,8 @@ def test_c_submatrix(pkg, oracle, synth, arm, wtol, k):
     assert maxnorm_rel(W, W64) < wtol
     assert maxnorm_rel(H, H64) < wtol
     assert_labels_match(lab, H64, oracle.classify)
-    # longer run: the divergence
-    _, _, _, kl = _run(pkg, V, k, arm, 200)
+    # final divergence, once it has settled
+    _, _, _, kl = _run(pkg, V, k, arm, KL_ITERS)
     assert abs(kl - kl64) <= 1e-5 * abs(kl64)
 
 
