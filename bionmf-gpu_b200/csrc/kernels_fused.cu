@@ -6,36 +6,45 @@
 // without ever materialising the n x m quotient:
 //
 //   TMA      : V tile (128 x BR, FP32) into a VST-deep ring; the Y tile
-//              (BR x KP, FP32) into a YST-deep ring; X (128 x KP, FP32) once.
+//              operands into a YST-deep ring.
 //   split    : k_split_factor, once per half-iteration, writes the other
-//              factor Y as TF32 hi + lo parts (hi = round-to-nearest TF32,
-//              lo = y - hi, exact) and as the transposed hi/lo blocks that MMA2
-//              reads K-major (an MN-major read of a TF32 operand returns zeros
-//              on sm_100a); the Y producer TMA-loads all three per tile, so no
-//              warp of the fused kernel splits Y.  X (128 rows per CTA) is split
-//              in place once per CTA by the accumulator warps.
-//   MMA1     : D (TMEM, 128 x BR, FP32) = Xl Yh^T + Xh Yl^T + Xh Yh^T
-//              (tcgen05.mma kind::tf32, A and B from shared memory, K-major).
+//              factor Y as TF32 hi (round to nearest) and the transposed hi/lo
+//              blocks that MMA2 reads K-major (lo = y - hi, exact; an MN-major
+//              read of a TF32 operand returns zeros on sm_100a), plus BF16
+//              copies bf16(lo), bf16(y) and bf16(y) transposed per tile; the Y
+//              producer TMA-loads them per tile.  X (128 rows per CTA) is split
+//              once per CTA by the accumulator warps.
+//   MMA1     : D (TMEM, 128 x BR) = Xh Yh^T                    (kind::tf32, k-steps of 8)
+//              + [bf16(Xh) | bf16(Xl)] [bf16(Yl) ; bf16(Y)]^T (kind::f16, K = 2 KP, k-steps of 16).
 //   epilogue : R = V / D in FP32 registers (V times an approximate reciprocal,
-//              <= 1.5 ulp; the reference uses fdividef),
-//              split R = Rh + Rl, written back to TMEM.
-//   MMA2     : Acc[tile] (TMEM, 128 x KP) = Rl Yh + Rh Yl + Rh Yh
-//              (kind::tf32, A = R from TMEM, B = Y^T from shared memory).
+//              <= 1.5 ulp; the reference uses fdividef);  R = Rh + Rl with
+//              Rh = TF32(R) written back over D and bf16(Rl) packed into a
+//              separate TMEM region.
+//   MMA2     : Acc[tile] (TMEM, 128 x 2 KP) = Rh [Yh | Yl]   (kind::tf32, N = 2 KP)
+//              + bf16(Rl) bf16(Y) into Acc[0:KP]               (kind::f16, K = 16).
 //   epilogue : adds Acc[tile] into FP32 registers (per-tile accumulation keeps
 //              the tensor core's FP32 sums short), and at the end writes the
 //              split's partial; k_factor (kernels_common.cu) sums the splits
 //              and applies X = X .* Xaux ./ colsum(Y).
 //
+// Precision of the two contractions: x y = xh yh + xh yl + xl y with xh, yh
+// TF32.  The large term xh yh (and, in MMA2, rh yl) is an exact TF32 product
+// with FP32 accumulation; the small terms, each at most 2^-12 of the whole,
+// are BF16 products (relative rounding 2^-9 of the term), so every product is
+// accurate to about 2^-20 relative.  Against the 3 x TF32 form (12 + 16 MMAs
+// per 64-column tile at k = 32, all at the tensor pipe's per-instruction floor
+// of N <= 64) this issues 8 + 12, and the R warps' epilogue stays one TMEM load
+// and one reciprocal per element.
+//
 // Reference equivalent: get_H_BLM / get_W_BLN (src/NMF_routines.c:376-525,
 // 1014-1164): two cuBLAS SGEMMs around matrix_div_sub with WH in HBM.
 //
 // Warp roles (512 threads): warp 0 = V producer (TMA), warp 1 = MMA issuer and
-// TMEM owner, warp 2 = X/Y producer (TMA), warps 4-11 = R warps (warp w reads
-// TMEM lanes 32*(w%4)..+31, column half (w-4)/4 of every tile), warps 12-15 =
-// accumulator and split warps.
+// TMEM owner, warp 2 = Y producer (TMA), warps 4-11 (or 4-19) = R warps (warp w
+// reads TMEM lanes 32*(w%4)..+31, column group (w-4)/4 of every tile),
+// last 4 warps = accumulator and split warps.
 // V stages are released as soon as the epilogue has read them, Y stages when
-// MMA1 has completed; a Y^T stage is rewritten only after the MMA2 that read
-// it has completed.
+// MMA2 (the last reader) has completed.
 // Every mbarrier wait is bounded (1 s of %globaltimer); on expiry the kernel
 // records an error word that the host turns into NMFB_ETIMEOUT.
 // No TMA multicast is used anywhere.
@@ -43,6 +52,7 @@
 #include "fused_common.cuh"
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <float.h>
 #include <cudaTypedefs.h>
 
@@ -51,12 +61,51 @@ using namespace nmfb_tc;
 
 namespace {
 
+// kind::f16 instruction descriptor with BF16 A and B (K-major) and FP32 D.
+__host__ __device__ constexpr uint32_t idesc_bf16xf32(uint32_t M, uint32_t N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// kind::f16 MMA with A from tensor memory (two BF16 per 32-bit column, the
+// lower K index in the low half) and B from shared memory.
+__device__ __forceinline__ void mma_ts_bf16(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// Two floats to a BF16 pair (round to nearest even), `first` in the low half.
+__device__ __forceinline__ uint32_t bf16x2_rn(float first, float second)
+{
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(second), "f"(first));
+    return r;
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t *r)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+// Swizzle of a K-major operand whose rows are `bytes` long: the UMMA layout code
+// and the tensor-map mode (rows of 32 / 64 / 128 bytes).
+__host__ __device__ constexpr uint32_t umma_layout(int bytes) { return bytes == 32 ? 6u : bytes == 64 ? 4u : 2u; }
+
 struct FusedMaps {
     CUtensorMap v;       // V, box [128 x BR] (H side, no swizzle) or [32 x 128] (W side, 128B swizzle)
-    CUtensorMap x;       // factor being updated (FP32, rows x KP), box rows = BO
     CUtensorMap y;       // TF32 hi part of the other factor (rows x KP), box rows = BR
-    CUtensorMap yl;      // its lo part (same layout)
     CUtensorMap yt;      // its transposed split: per 32 rows, [hi^T (KP x 32) ; lo^T (KP x 32)]
+    CUtensorMap ylb;     // BF16 copy of its lo part (rows x KP), box [KP x BR]
+    CUtensorMap yb;      // BF16 copy (rows x KP), box [KP x BR]
+    CUtensorMap ybt;     // BF16 transposed tiles: per BR rows, KP rows of BR values; box [BR x KP]
 };
 
 struct FusedArgs {
@@ -80,65 +129,92 @@ struct Geo {
     static constexpr int NB = KP / CB;                     // column blocks
     static constexpr int ROWB = CB * 4;                    // bytes per row of a block
     static constexpr uint32_t LAYOUT = (KP == 16) ? 4u : 2u;  // SW64 : SW128
-    static constexpr int YBLK = BR * ROWB;                 // bytes of one Y column block
+    static constexpr int YBLK = BR * ROWB;                 // bytes of one Yh column block
     static constexpr int YTBLK = KP * 128;                 // bytes of one Y^T part (32 reduction rows)
     static constexpr int YTPAIR = 2 * YTBLK;               // Y^T hi part followed by its lo part
     static constexpr int YBYTES = BR * KP * 4;
     static constexpr int VBYTES = BO * BR * 4;
-    static constexpr int YSTAGE = 2 * YBYTES;              // Yh (TMA target, split in place) | Yl
-    static constexpr int YTSTAGE = 2 * YBYTES;             // YTh | YTl
+    static constexpr int YSTAGE = YBYTES;                  // Yh (TF32), NB column blocks
+    static constexpr int YTSTAGE = 2 * YBYTES;             // YTh | YTl (per 32 rows)
+    static constexpr int YBB = BR * KP * 2;                // one BF16 tile of BR rows of 2 KP bytes
+    static constexpr int YBTB = KP * BR * 2;               // bf16(Y)^T tile, KP rows of 2 BR bytes
+    static constexpr int YBSTAGE = 2 * YBB + YBTB;         // bf16(Yl) | bf16(Y) | bf16(Y)^T
+    static constexpr uint32_t BLAYOUT = umma_layout(2 * KP);
+    static constexpr uint32_t BTLAYOUT = umma_layout(2 * BR);
     static constexpr int YST = 3;
     static constexpr int FIXED = 1024 + 512;
-    static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YST * (YSTAGE + YTSTAGE)) / VBYTES;
+    static constexpr int YALL = YST * (YSTAGE + YTSTAGE + YBSTAGE);
+    static constexpr int VAVAIL = (SMEM_LIMIT - FIXED - YALL) / VBYTES;
     static constexpr int VST = VAVAIL > 6 ? 6 : VAVAIL;    // V ring depth (HBM stream)
-    static constexpr int SMEM = FIXED + YST * (YSTAGE + YTSTAGE) + VST * VBYTES;
-    static_assert(VST >= 2, "shared-memory ring too small");
+    static constexpr int SMEM = FIXED + YALL + VST * VBYTES;
+    static_assert(VST >= 3, "shared-memory ring too small");
+    static_assert(YBB % 1024 == 0 && YBSTAGE % 1024 == 0 && YSTAGE % 1024 == 0, "1024-byte stage alignment");
     static constexpr int NR = (KP >= 64) ? 8 : 16;        // R warps
     static constexpr int QW = BR / (NR / 4);               // tile columns per R warp
+    static_assert(QW == 16, "one BF16 k-step (16 columns) per R-warp column group");
     static constexpr int NTHR = (4 + NR + 4) * 32;
     static constexpr uint32_t ACC = 2 * KP;                // TMEM columns of one per-tile accumulator
-    static constexpr uint32_t DB0 = 2 * ACC;               // first D buffer column
-    static constexpr uint32_t NDB = (KP == 16) ? 3 : 2;    // D buffers (MMA1 runs NDB tiles ahead)
-    static constexpr uint32_t XC0 = DB0 + NDB * 2 * BR;    // X hi at XC0, X lo at XC0 + KP
-    static_assert(XC0 + 2 * KP <= 512, "TMEM columns exceeded");
+    static constexpr uint32_t NDB = (KP == 16) ? 4 : (KP == 32) ? 3 : 2;   // D buffers (MMA1 runs NDB tiles ahead)
+    static constexpr uint32_t DA0 = 2 * ACC;               // D[b] (then Rh[b]) at DA0 + b BR
+    static constexpr uint32_t RL0 = DA0 + NDB * BR;        // bf16(Rl)[b] at RL0 + b BR/2
+    static constexpr uint32_t XC0 = RL0 + NDB * BR / 2;    // X hi (TF32), KP columns
+    static constexpr uint32_t XB0 = XC0 + KP;              // bf16(X hi) | bf16(X lo), KP/2 columns each
+    static_assert(XB0 + KP <= 512, "TMEM columns exceeded");
 };
 
-// TMEM columns: per-tile accumulators Acc[b] at b*2KP (2KP columns: the Rh Y^T_hi
-// + Rl Y^T_hi sum and the Rh Y^T_lo part side by side), D[b] (later Rh[b]) at
-// 4KP + b*2*BR, Rl[b] at 4KP + b*2*BR + BR, b < NDB; then the CTA's 128 rows of
-// X as TF32 hi (KP columns) and lo (KP columns), the A operand of MMA1 for every
-// tile (so MMA1 reads only Y from shared memory).
+// TMEM columns: per-tile accumulators Acc[b] at b*2KP (2KP columns: the Rh Yh +
+// bf16(Rl) bf16(Y) sum and the Rh Yl part side by side); D[b] (BR columns, then
+// Rh[b]) at DA0 + b*BR and bf16(Rl)[b] (BR/2 columns, column group g of 16 in
+// its 8 columns RL0 + b*BR/2 + 8g), b < NDB; then the CTA's 128 rows of X as
+// TF32 hi (KP columns) and bf16(X hi) | bf16(X lo) (KP/2 columns each), the A
+// operands of MMA1 for every tile (so MMA1 reads only Y from shared memory).
 
 // Split a factor Y (rows x kp, FP32, padding columns zero) for the fused
-// kernel's TMA loads: hi = TF32(y) (round to nearest), lo = y - hi (exact),
-// both rows x kp; and per block of 32 rows the transposed hi block (kp rows of
-// 32 floats) followed by the transposed lo block, rows past the end zero.
-// One CTA per 32-row block; the transpose goes through shared memory.
+// kernel's TMA loads, one CTA per block of `br` rows (br = the kernel's tile):
+//   hi = TF32(y) (round to nearest), rows x kp;
+//   T: per 32 rows, the transposed hi block (kp rows of 32 floats) followed by
+//      the transposed lo block (lo = y - hi, exact), rows past the end zero;
+//   Bl = bf16(lo), B = bf16(y): rows x kp each;
+//   BT: per br rows, the transposed bf16(y) block (kp rows of br values), rows
+//      past the end zero.
+// The transposes go through shared memory.
 __global__ void __launch_bounds__(256) k_split_factor(const float *__restrict__ Y, uint32_t rows, uint32_t kp,
-                                                      float *__restrict__ hi, float *__restrict__ lo,
-                                                      float *__restrict__ T, const ConvState *st)
+                                                      uint32_t br, float *__restrict__ hi, float *__restrict__ T,
+                                                      __nv_bfloat16 *__restrict__ Bl, __nv_bfloat16 *__restrict__ B,
+                                                      __nv_bfloat16 *__restrict__ BT, const ConvState *st)
 {
     if (st && *(volatile const uint32_t *)&st->converged) return;
-    __shared__ float th[32][65], tl[32][65];
-    uint32_t const r0 = blockIdx.x * 32;
-    for (uint32_t e = threadIdx.x; e < 32 * kp; e += blockDim.x) {
+    __shared__ float th[64][65], tl[64][65];
+    __shared__ __nv_bfloat16 tb[64][66];
+    uint32_t const r0 = blockIdx.x * br;
+    for (uint32_t e = threadIdx.x; e < br * kp; e += blockDim.x) {
         uint32_t const r = e / kp, c = e % kp;
         bool const in = r0 + r < rows;
         float const y = in ? Y[(size_t)(r0 + r) * kp + c] : 0.0f;
         float const h = tf32_rna(y), l = y - h;
+        __nv_bfloat16 const yb = __float2bfloat16_rn(y);
         if (in) {
             hi[(size_t)(r0 + r) * kp + c] = h;
-            lo[(size_t)(r0 + r) * kp + c] = l;
+            Bl[(size_t)(r0 + r) * kp + c] = __float2bfloat16_rn(l);
+            B[(size_t)(r0 + r) * kp + c] = yb;
         }
         th[r][c] = h;
         tl[r][c] = l;
+        tb[r][c] = yb;
     }
     __syncthreads();
-    float *dst = T + (size_t)blockIdx.x * 2 * kp * 32;
-    for (uint32_t e = threadIdx.x; e < 2 * kp * 32; e += blockDim.x) {
-        uint32_t const row = e / 32, rr = e % 32;
-        dst[e] = row < kp ? th[rr][row] : tl[rr][row - kp];
+    uint32_t const nblk32 = (rows + 31) / 32;
+    for (uint32_t sub = 0; sub < br / 32; sub++) {
+        uint32_t const blk = r0 / 32 + sub;
+        if (blk >= nblk32) break;
+        float *dst = T + (size_t)blk * 2 * kp * 32;
+        for (uint32_t e = threadIdx.x; e < 2 * kp * 32; e += blockDim.x) {
+            uint32_t const row = e / 32, rr = sub * 32 + e % 32;
+            dst[e] = row < kp ? th[rr][row] : tl[rr][row - kp];
+        }
     }
+    __nv_bfloat16 *bt = BT + (size_t)blockIdx.x * kp * br;
+    for (uint32_t e = threadIdx.x; e < kp * br; e += blockDim.x) bt[e] = tb[e % br][e / br];
 }
 
 // Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X and Y
@@ -154,7 +230,6 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     constexpr int QW = G::QW;           // tile columns handled by one R warp
     constexpr int NR = G::NR;
     constexpr uint32_t ACC_COLS = G::ACC;
-    constexpr uint32_t DBUF0 = G::DB0;
     if (args.st && *(volatile const uint32_t *)&args.st->converged) return;
 
     extern __shared__ unsigned char smem_raw[];
@@ -162,7 +237,8 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     unsigned char *const base = smem_raw + (base_u32 - smem_u32(smem_raw));
     unsigned char *const sY = base;                                 // [YST][Yh | Yl]
     unsigned char *const sYT = sY + G::YST * G::YSTAGE;             // [YST][YTh | YTl]
-    unsigned char *const sV = sYT + G::YST * G::YTSTAGE;            // [VST][VBYTES]
+    unsigned char *const sYB = sYT + G::YST * G::YTSTAGE;           // [YST][bf16 Y | bf16 Y^T]
+    unsigned char *const sV = sYB + G::YST * G::YBSTAGE;            // [VST][VBYTES]
     uint64_t *const bars = reinterpret_cast<uint64_t *>(sV + G::VST * G::VBYTES);
     uint64_t *const vfull = bars;                   // [VST]  TMA -> epilogue
     uint64_t *const vempty = vfull + G::VST;        // [VST]  epilogue -> V producer
@@ -280,11 +356,14 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                 unsigned char *syh = sY + s * G::YSTAGE;
                 int const r0 = (int)((t_begin + t) * BR);
                 DBG_TS(1, t);
-                mbar_expect_tx(&yfull[s], (NTERMS == 3 ? 2 : 1) * G::YBYTES + G::YTSTAGE);
+                mbar_expect_tx(&yfull[s], G::YBYTES + G::YTSTAGE + (NTERMS == 3 ? G::YBSTAGE : 0));
                 for (int b = 0; b < G::NB; b++) tma_load_2d(syh + b * G::YBLK, &maps.y, &yfull[s], b * G::CB, r0, pol);
-                if (NTERMS == 3)
-                    for (int b = 0; b < G::NB; b++)
-                        tma_load_2d(syh + G::YBYTES + b * G::YBLK, &maps.yl, &yfull[s], b * G::CB, r0, pol);
+                if (NTERMS == 3) {
+                    unsigned char *syb = sYB + s * G::YBSTAGE;
+                    tma_load_2d(syb, &maps.ylb, &yfull[s], 0, r0, pol);
+                    tma_load_2d(syb + G::YBB, &maps.yb, &yfull[s], 0, r0, pol);
+                    tma_load_2d(syb + 2 * G::YBB, &maps.ybt, &yfull[s], 0, (int)((t_begin + t) * KP), pol);
+                }
                 // Y^T: the BR / 32 row blocks of this tile, 2 KP rows of 128 B each
                 tma_load_2d(sYT + s * G::YTSTAGE, &maps.yt, &yfull[s], 0, (r0 / 32) * 2 * KP, pol);
             }
@@ -301,13 +380,17 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         // The Y stage of tile t is released when MMA2(t), the last reader, completes.
         if (lane == 0) {
             constexpr uint32_t IDESC1 = idesc_tf32(BO, BR, 0);
+            constexpr uint32_t IDESC1B = idesc_bf16xf32(BO, BR);
             constexpr uint32_t IDESC2 = idesc_tf32(BO, KP, 0);
             constexpr uint32_t IDESC2W = idesc_tf32(BO, 2 * KP, 0);
+            constexpr uint32_t IDESC2B = idesc_bf16xf32(BO, KP);
             // Shared-memory descriptors are built once; a k-step or stage offset is
             // added to the start-address field (16-byte units, no carry out of it:
             // every operand lies below 256 KB).
             uint64_t const dY0 = smem_desc(smem_u32(sY), 16, 8 * G::ROWB, G::LAYOUT);
             uint64_t const dYT0 = smem_desc(smem_u32(sYT), 16, 1024, 2u);
+            uint64_t const dYB0 = smem_desc(smem_u32(sYB), 16, 8 * 2 * KP, G::BLAYOUT);
+            uint64_t const dYBT0 = smem_desc(smem_u32(sYB + 2 * G::YBB), 16, 8 * 2 * BR, G::BTLAYOUT);
             bool ok = mbar_wait(xready, 0, abort_flag, args.err, 3u, args.wait_ns);
             tc_fence_after();
             uint32_t n1 = 0, n2 = 0;
@@ -319,23 +402,24 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                     tc_fence_after();
                     uint32_t const sp = n2 % G::YST, bp = n2 & 1, db = n2 % G::NDB;
                     uint64_t const dYT = dYT0 + ((sp * G::YTSTAGE) >> 4);
-                    uint32_t const rh = tmem + DBUF0 + db * 2 * BR;
-                    uint32_t const rl = rh + BR;
+                    uint32_t const rh = tmem + G::DA0 + db * BR;
+                    uint32_t const rl = tmem + G::RL0 + db * (BR / 2);
                     uint32_t const dacc = tmem + bp * ACC_COLS;
-                    // MMA2 for this tile only, K = BR reduction rows in steps of 8:
-                    //   Acc[bp][0:2KP] (+)= Rh [Y^T_hi; Y^T_lo]   (one MMA, N = 2 KP)
-                    //   Acc[bp][0:KP]   += Rl Y^T_hi              (N = KP)
-                    // so Acc[0:KP] + Acc[KP:2KP] = Rh Yh + Rl Yh + Rh Yl (summed by the
+                    // MMA2 for this tile only, K = BR reduction rows:
+                    //   Acc[bp][0:2KP] (+)= Rh [Y^T_hi; Y^T_lo]     (kind::tf32, N = 2 KP, k-steps of 8)
+                    //   Acc[bp][0:KP]   += bf16(Rl) bf16(Y)^T      (kind::f16, N = KP, k-steps of 16;
+                    //                      column group g of the R warps = k-step g, A at rl + 8 g)
+                    // so Acc[0:KP] + Acc[KP:2KP] = Rh Yh + Rh Yl + Rl Y (summed by the
                     // accumulator warps in FP32 registers).
 #pragma unroll
                     for (int ks = 0; ks < BR / 8; ks++) {
                         uint32_t const ob = ((ks / 4) * G::YTPAIR + (ks % 4) * 32) >> 4;
-                        if (NTERMS == 3) {
-                            mma_ts(dacc, rh + ks * 8, dYT + ob, IDESC2W, ks > 0 ? 1u : 0u);
-                            mma_ts(dacc, rl + ks * 8, dYT + ob, IDESC2, 1u);
-                        } else {
-                            mma_ts(dacc, rh + ks * 8, dYT + ob, IDESC2, ks > 0 ? 1u : 0u);
-                        }
+                        mma_ts(dacc, rh + ks * 8, dYT + ob, NTERMS == 3 ? IDESC2W : IDESC2, ks > 0 ? 1u : 0u);
+                    }
+                    if (NTERMS == 3) {
+                        uint64_t const dYBT = dYBT0 + ((sp * G::YBSTAGE) >> 4);
+#pragma unroll
+                        for (int g = 0; g < BR / 16; g++) mma_ts_bf16(dacc, rl + g * 8, dYBT + g * 2, IDESC2B, 1u);
                     }
                     tc_commit(&accrdy[bp]);
                     tc_commit(&yempty[sp]);
@@ -347,19 +431,23 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                     tc_fence_after();
                     uint32_t const s = n1 % G::YST, db = n1 % G::NDB;
                     uint64_t const dYh = dY0 + ((s * G::YSTAGE) >> 4);
-                    uint64_t const dYl = dYh + (G::YBYTES >> 4);
-                    uint32_t const dcol = tmem + DBUF0 + db * 2 * BR;
-                    // MMA1: D = Xl Yh^T + Xh Yl^T + Xh Yh^T (small terms first), K = KP in steps of 8.
+                    uint32_t const dcol = tmem + G::DA0 + db * BR;
+                    uint32_t const xh = tmem + G::XC0;
+                    // MMA1, K = KP:  D = Xh Yh^T (TF32, k-steps of 8 per column block), then
+                    // D += [bf16(Xh) | bf16(Xl)] [bf16(Yl) ; bf16(Y)]^T (K = 2 KP, k-steps of 16:
+                    // the first KP / 16 read bf16(Yl), the rest bf16(Y)).
 #pragma unroll
-                    for (int tt = 0; tt < NTERMS; tt++) {
-                        int const term = NTERMS - 1 - tt;   // 2: Xl*Yh, 1: Xh*Yl, 0: Xh*Yh
-                        uint32_t const xa = tmem + G::XC0 + ((term == 2) ? KP : 0);
-                        uint64_t const yb = (term == 1) ? dYl : dYh;
+                    for (int ks = 0; ks < KP / 8; ks++) {
+                        constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
+                        uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
+                        mma_ts(dcol, xh + ks * 8, dYh + ob, IDESC1, ks > 0 ? 1u : 0u);
+                    }
+                    if (NTERMS == 3) {
+                        uint64_t const dYB = dYB0 + ((s * G::YBSTAGE) >> 4);
 #pragma unroll
-                        for (int ks = 0; ks < KP / 8; ks++) {
-                            constexpr int KPB = G::CB / 8;     // k-steps per swizzle column block
-                            uint32_t const ob = ((ks / KPB) * G::YBLK + (ks % KPB) * 32) >> 4;
-                            mma_ts(dcol, xa + ks * 8, yb + ob, IDESC1, (tt > 0 || ks > 0) ? 1u : 0u);
+                        for (int j = 0; j < KP / 8; j++) {
+                            uint32_t const ob = ((j / (KP / 16)) * G::YBB + (j % (KP / 16)) * 32) >> 4;
+                            mma_ts_bf16(dcol, tmem + G::XB0 + j * 8, dYB + ob, IDESC1B, 1u);
                         }
                     }
                     tc_commit(&dfull[db]);
@@ -400,13 +488,11 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             DBG_PH(2, t);
             if (warp == 4 && lane == 0) DBG_TS(5, t);
             const unsigned char *sv = sV + s * G::VBYTES;
-            uint32_t const dcol = DBUF0 + b * 2 * BR + half * QW;
+            uint32_t const dcol = G::DA0 + b * BR + half * QW;        // this group's columns of D
+            uint32_t const rlcol = G::RL0 + b * (BR / 2) + half * 8;  // and of bf16(Rl)
             uint32_t d[32];   // D, then the TF32 hi part of R
             uint32_t v[32];   // V, then the lo part of R
-            if (QW == 32)
-                tmem_ld32(lane_addr + dcol, d);
-            else
-                tmem_ld16(lane_addr + dcol, d);
+            tmem_ld16(lane_addr + dcol, d);
             if (HSIDE) {
                 // V tile [BR rows][128 cols], row-major; this thread's column = row.
                 const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
@@ -440,17 +526,19 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             DBG_PH(3, t);
             tmem_wait_ld_dep(d);
             DBG_PH(4, t);
+            uint32_t pl[8];   // bf16(R lo), packed in column pairs
 #pragma unroll
             for (int c = 0; c < QW; c++) {
                 // R = V / WH as V * (1/WH): the approximate reciprocal (<= 1 ulp) runs at
                 // full rate, the fast-division intrinsic at a third of it.  min(., FLT_MAX)
                 // keeps the zero-filled edges (V = 0, WH = 0) at 0 instead of 0 * inf.
                 float const vv = __uint_as_float(v[c]);
-                float const r = vv * fminf(rcp_approx(__uint_as_float(d[c])), FLT_MAX);
+                float const wh = __uint_as_float(d[c]);
+                float const r = vv * fminf(rcp_approx(wh), FLT_MAX);
                 float const h = tf32_rna(r);
 #ifdef NMFB_FUSED_DEBUG
                 if (args.dbg && blockIdx.x == 0 && t == 0) {
-                    args.dbg[row * 64 + half * QW + c] = __uint_as_float(d[c]);
+                    args.dbg[row * 64 + half * QW + c] = wh;
                     args.dbg[BO * 64 + row * 64 + half * QW + c] = vv;
                     args.dbg[2 * BO * 64 + row * 64 + half * QW + c] = h;
                 }
@@ -458,14 +546,13 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                 d[c] = __float_as_uint(h);
                 v[c] = __float_as_uint(r - h);
             }
-            DBG_PH(5, t);
-            if (QW == 32) {
-                tmem_st32(lane_addr + dcol, d);
-                if (NTERMS == 3) tmem_st32(lane_addr + dcol + BR, v);
-            } else {
-                tmem_st16(lane_addr + dcol, d);
-                if (NTERMS == 3) tmem_st16(lane_addr + dcol + BR, v);
+            if (NTERMS == 3) {
+#pragma unroll
+                for (int j = 0; j < QW / 2; j++) pl[j] = bf16x2_rn(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
             }
+            DBG_PH(5, t);
+            tmem_st16(lane_addr + dcol, d);
+            if (NTERMS == 3) tmem_st8(lane_addr + rlcol, pl);
             tmem_wait_st();
             DBG_PH(6, t);
             tc_fence_before();
@@ -488,26 +575,34 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
 #pragma unroll
         for (int c = 0; c < KP; c++) sum[c] = 0.0f;
         bool ok = true;
-        {   // this thread's row of X, split into TF32 hi / lo, into TMEM lanes = rows
+        {   // this thread's row of X as TF32 hi and bf16(hi) | bf16(lo), into TMEM lanes = rows
             uint32_t const o = o0 + row;
             const float *xr = args.X + (size_t)o * KP;
 #pragma unroll
             for (int c0 = 0; c0 < KP; c0 += 16) {
-                uint32_t h[32], l[32];
+                uint32_t h[32], hb[8], lb[8];
 #pragma unroll
                 for (int c = 0; c < 16; c += 4) {
                     float4 const x = (o < args.O) ? *reinterpret_cast<const float4 *>(xr + c0 + c)
                                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     float const xs[4] = {x.x, x.y, x.z, x.w};
+                    float hv[4], lo[4];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        float const hv = tf32_rna(xs[i]);
-                        h[c + i] = __float_as_uint(hv);
-                        l[c + i] = __float_as_uint(xs[i] - hv);
+                        hv[i] = tf32_rna(xs[i]);
+                        h[c + i] = __float_as_uint(hv[i]);
+                        lo[i] = xs[i] - hv[i];
                     }
+                    hb[c / 2] = bf16x2_rn(hv[0], hv[1]);
+                    hb[c / 2 + 1] = bf16x2_rn(hv[2], hv[3]);
+                    lb[c / 2] = bf16x2_rn(lo[0], lo[1]);
+                    lb[c / 2 + 1] = bf16x2_rn(lo[2], lo[3]);
                 }
                 tmem_st16(lane_addr + G::XC0 + c0, h);
-                tmem_st16(lane_addr + G::XC0 + KP + c0, l);
+                if (NTERMS == 3) {
+                    tmem_st8(lane_addr + G::XB0 + c0 / 2, hb);
+                    tmem_st8(lane_addr + G::XB0 + KP / 2 + c0 / 2, lb);
+                }
             }
             tmem_wait_st();
             tc_fence_before();
@@ -584,8 +679,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-int encode_2d(nmfb_ctx *ctx, CUtensorMap *map, const float *base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
-              uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw)
+int encode_2d(nmfb_ctx *ctx, CUtensorMap *map, const void *base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+              uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw,
+              CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32)
 {
     auto fn = encode_fn();
     if (!fn) return nmfb_fail(ctx, NMFB_ENODEV, "cuTensorMapEncodeTiled unavailable");
@@ -593,17 +689,37 @@ int encode_2d(nmfb_ctx *ctx, CUtensorMap *map, const float *base, uint64_t inner
     cuuint64_t strides[1] = {row_bytes};
     cuuint32_t box[2] = {box_inner, box_outer};
     cuuint32_t es[2] = {1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
+    CUresult r = fn(map, dt, 2, (void *)base, dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return nmfb_fail(ctx, NMFB_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return NMFB_OK;
 }
 
+// Layout of one factor's split copies (k_split_factor's outputs), in one buffer:
+// hi (rows x kp FP32) | transposed hi/lo per 32 rows | bf16(lo) (rows x kp) |
+// bf16(y) (rows x kp) | bf16(y) transposed per br rows.
+struct SplitLayout {
+    size_t t, bl, b, bt, floats;   // offsets in floats (bl, b, bt: start of the BF16 parts)
+    uint32_t br, nblk32, nblkbr;
+    SplitLayout(uint32_t rows, uint32_t kp)
+    {
+        br = (kp >= 64) ? 32 : 64;
+        nblk32 = (rows + 31) / 32;
+        nblkbr = (rows + br - 1) / br;
+        size_t const f = (size_t)rows * kp;
+        t = f;
+        bl = t + (size_t)nblk32 * 64 * kp;
+        b = bl + f / 2;                                   // rows * kp BF16 = f / 2 floats (kp is even)
+        bt = b + f / 2;
+        floats = bt + ((size_t)nblkbr * kp * br + 1) / 2;
+    }
+};
+
 struct FusedPlan {
     FusedMaps mapsH, mapsW;  // update_H (HSIDE) and update_W
     uint32_t *dErr;
-    float *dSplitW, *dSplitH;  // hi | lo | transposed blocks of W and of H (k_split_factor)
+    float *dSplitW, *dSplitH;  // split copies of W and of H (k_split_factor, SplitLayout)
 #ifdef NMFB_FUSED_DEBUG
     float *dDbg;
 #endif
@@ -688,9 +804,11 @@ int fused_half(nmfb_ctx *ctx, bool is_H, int adjust)
     if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
     {
         float *sp = is_H ? plan->dSplitW : plan->dSplitH;
-        size_t const part = (size_t)yrows * ctx->kp;
-        k_split_factor<<<(yrows + 31) / 32, 256, 0, ctx->stream>>>(Y, yrows, ctx->kp, sp, sp + part, sp + 2 * part,
-                                                                   ctx->dState);
+        SplitLayout const L(yrows, ctx->kp);
+        k_split_factor<<<L.nblkbr, 256, 0, ctx->stream>>>(Y, yrows, ctx->kp, L.br, sp, sp + L.t,
+                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.bl),
+                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.b),
+                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.bt), ctx->dState);
         NMFB_LAUNCH_CHECK(ctx);
     }
     int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH) : dispatch<false>(ctx, plan->mapsW);
@@ -733,33 +851,37 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
 #endif
     uint32_t const cb = (kp == 16) ? 16 : 32;
     CUtensorMapSwizzle const fsw = (kp == 16) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    auto const sw_for = [](uint32_t bytes) {
+        return bytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    };
+    CUtensorMapDataType const BF16 = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     uint64_t const vrow = ctx->ldv * sizeof(float), frow = (uint64_t)kp * sizeof(float);
-    uint32_t const br = (kp >= 64) ? 32 : 64;
-    // Split copies of W and H: hi (rows x kp) | lo (rows x kp) | transposed blocks
-    // (ceil(rows / 32) blocks of 2 kp x 32 floats).
-    size_t const wsz = (size_t)ctx->n * kp, hsz = (size_t)ctx->m * kp;
-    uint32_t const wblk = (ctx->n + 31) / 32, hblk = (ctx->m + 31) / 32;
-    e = nmfb_malloc(ctx, (void **)&plan->dSplitW, (2 * wsz + (size_t)wblk * 64 * kp) * sizeof(float));
-    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, (2 * hsz + (size_t)hblk * 64 * kp) * sizeof(float));
+    SplitLayout const LW(ctx->n, kp), LH(ctx->m, kp);
+    uint32_t const br = LW.br;
+    e = nmfb_malloc(ctx, (void **)&plan->dSplitW, LW.floats * sizeof(float));
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, LH.floats * sizeof(float));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused split buffers: %s", cudaGetErrorString(e));
+    // Maps over one factor's split copies: Y (the other factor, `rows` rows).
+    auto const y_maps = [&](FusedMaps &mp, const float *sp, const SplitLayout &L, uint32_t rows) -> int {
+        int r;
+        if ((r = encode_2d(ctx, &mp.y, sp, kp, rows, frow, cb, br, fsw))) return r;
+        if ((r = encode_2d(ctx, &mp.ylb, sp + L.bl, kp, rows, (uint64_t)kp * 2, kp, br, sw_for(2 * kp), BF16)))
+            return r;
+        if ((r = encode_2d(ctx, &mp.yt, sp + L.t, 32, (uint64_t)L.nblk32 * 2 * kp, 128, 32, 2 * kp * (br / 32),
+                           CU_TENSOR_MAP_SWIZZLE_128B)))
+            return r;
+        if ((r = encode_2d(ctx, &mp.yb, sp + L.b, kp, rows, (uint64_t)kp * 2, kp, br, sw_for(2 * kp), BF16))) return r;
+        return encode_2d(ctx, &mp.ybt, sp + L.bt, br, (uint64_t)L.nblkbr * kp, (uint64_t)br * 2, br, kp,
+                         sw_for(2 * br), BF16);
+    };
     // update_H: X = H (rows m), Y = W (rows n); V tile [br rows of V][128 cols].
     FusedMaps &mh = plan->mapsH;
     if ((rc = encode_2d(ctx, &mh.v, ctx->dV, ctx->m, ctx->n, vrow, BO, br, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
-    if ((rc = encode_2d(ctx, &mh.x, ctx->dH, kp, ctx->m, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.y, plan->dSplitW, kp, ctx->n, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.yl, plan->dSplitW + wsz, kp, ctx->n, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mh.yt, plan->dSplitW + 2 * wsz, 32, (uint64_t)wblk * 2 * kp, 128, 32, 2 * kp * (br / 32),
-                        CU_TENSOR_MAP_SWIZZLE_128B)))
-        return rc;
+    if ((rc = y_maps(mh, plan->dSplitW, LW, ctx->n))) return rc;
     // update_W: X = W (rows n), Y = H (rows m); V tile [128 rows][32 cols] x (br/32), 128B swizzle.
     FusedMaps &mw = plan->mapsW;
     if ((rc = encode_2d(ctx, &mw.v, ctx->dV, ctx->m, ctx->n, vrow, 32, BO, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode_2d(ctx, &mw.x, ctx->dW, kp, ctx->n, frow, cb, BO, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.y, plan->dSplitH, kp, ctx->m, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.yl, plan->dSplitH + hsz, kp, ctx->m, frow, cb, br, fsw))) return rc;
-    if ((rc = encode_2d(ctx, &mw.yt, plan->dSplitH + 2 * hsz, 32, (uint64_t)hblk * 2 * kp, 128, 32, 2 * kp * (br / 32),
-                        CU_TENSOR_MAP_SWIZZLE_128B)))
-        return rc;
+    if ((rc = y_maps(mw, plan->dSplitH, LH, ctx->m))) return rc;
     return NMFB_OK;
 }
 
