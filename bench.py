@@ -408,8 +408,16 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
     seeds = np.tile(np.arange(1, R + 1, dtype=np.uint32), len(ks))
     nprob = len(ranks)
     flush = flush or L2Flush(dev)
+    # tile shapes per rank from the project's autotuner (timed short runs of a
+    # full wave per rank; cached per (k, m, n) bucket)
+    import nmf_b200.sweep as sweep
+    t0 = time.perf_counter()
+    tiles = sweep.autotune(V, ks, device=dev.index or 0)
+    tune_s = time.perf_counter() - t0
     dev_ms, e2e_ms, iters, ctas = [], [], None, 1
     with pkg.Batch(n, m, ranks, device=dev.index or 0) as b:
+        for p, k in enumerate(ranks):
+            b.set_tiles(p, *tiles[int(k)])
         for s in range(warmup + steps):
             torch.cuda.synchronize()
             flush()
@@ -447,7 +455,8 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
             "sequential": {"value": seq, "unit": "solves/s", "sample": f"{seq_n} solves (k=2..10 x {seq_sample} seeds), "
                                                                       "single-problem engine, host-timed"},
             "speedup_vs_sequential": batched / seq, "tflops": flops / (statistics.median(dev_ms) / 1e3) / 1e12,
-            "mean_iterations": float(np.mean(iters)), "ctas_per_problem": ctas, "cophenetic": {str(k): round(v, 6) for k, v in coph.items()},
+            "mean_iterations": float(np.mean(iters)), "ctas_per_problem": ctas,
+            "tiles": {str(k): list(v) for k, v in sorted(tiles.items())}, "autotune_s": round(tune_s, 2), "cophenetic": {str(k): round(v, 6) for k, v in coph.items()},
             "l2": "256 MB buffer written before every sweep"}
 
 

@@ -23,9 +23,11 @@
 //   MMA2     : Acc[tile] (TMEM, 128 x 2 KP) = Rh [Yh | Yl]   (kind::tf32, N = 2 KP)
 //              + bf16(Rl) bf16(Y) into Acc[0:KP]               (kind::f16, K = 16).
 //   epilogue : adds Acc[tile] into FP32 registers (per-tile accumulation keeps
-//              the tensor core's FP32 sums short), and at the end writes the
-//              split's partial; k_factor (kernels_common.cu) sums the splits
-//              and applies X = X .* Xaux ./ colsum(Y).
+//              the tensor core's FP32 sums short) and writes the split's
+//              partial; k_finish (one CTA per 128 rows) sums the splits, applies
+//              X = X .* Xaux ./ colsum(Y) (and the EPS adjust when asked), and
+//              writes X's split copies and column sums for the next
+//              half-iteration: two launches per half-iteration.
 //
 // Precision of the two contractions: x y = xh yh + xh yl + xl y with xh, yh
 // TF32.  The large term xh yh (and, in MMA2, rh yl) is an exact TF32 product
@@ -39,10 +41,10 @@
 // Reference equivalent: get_H_BLM / get_W_BLN (src/NMF_routines.c:376-525,
 // 1014-1164): two cuBLAS SGEMMs around matrix_div_sub with WH in HBM.
 //
-// Warp roles (512 threads): warp 0 = V producer (TMA), warp 1 = MMA issuer and
-// TMEM owner, warp 2 = Y producer (TMA), warps 4-11 (or 4-19) = R warps (warp w
-// reads TMEM lanes 32*(w%4)..+31, column group (w-4)/4 of every tile),
-// last 4 warps = accumulator and split warps.
+// Warp roles: warp 0 = V producer (TMA), warp 1 = MMA issuer and TMEM owner,
+// warp 2 = Y producer (TMA), warps 4-11 (or 4-19) = R warps in two teams that
+// take alternate tiles (warp w reads TMEM lanes 32*(w%4)..+31), last 4 warps =
+// accumulator and split warps.
 // V stages are released as soon as the epilogue has read them, Y stages when
 // MMA2 (the last reader) has completed.
 // Every mbarrier wait is bounded (1 s of %globaltimer); on expiry the kernel
@@ -94,6 +96,8 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t *r)
                  "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
                  : "memory");
 }
+
+constexpr uint32_t ECH = 32;   // row blocks per chunk of k_finish's column sums
 
 // Swizzle of a K-major operand whose rows are `bytes` long: the UMMA layout code
 // and the tensor-map mode (rows of 32 / 64 / 128 bytes).
@@ -150,8 +154,6 @@ struct Geo {
     static_assert(VST >= 3, "shared-memory ring too small");
     static_assert(YBB % 1024 == 0 && YBSTAGE % 1024 == 0 && YSTAGE % 1024 == 0, "1024-byte stage alignment");
     static constexpr int NR = (KP >= 64) ? 8 : 16;        // R warps
-    static constexpr int QW = BR / (NR / 4);               // tile columns per R warp
-    static_assert(QW == 16, "one BF16 k-step (16 columns) per R-warp column group");
     static constexpr int NTHR = (4 + NR + 4) * 32;
     static constexpr uint32_t ACC = 2 * KP;                // TMEM columns of one per-tile accumulator
     static constexpr uint32_t NDB = (KP == 16) ? 4 : (KP == 32) ? 3 : 2;   // D buffers (MMA1 runs NDB tiles ahead)
@@ -217,6 +219,189 @@ __global__ void __launch_bounds__(256) k_split_factor(const float *__restrict__ 
     for (uint32_t e = threadIdx.x; e < kp * br; e += blockDim.x) bt[e] = tb[e % br][e / br];
 }
 
+// Finish of a half-iteration, one CTA of 512 threads per 128-row block of X
+// (four threads per row, a quarter of its columns each), right after k_fused_half:
+//   Xaux = the split partials summed in split order; X = X * Xaux / accY
+//   (matrix_mul_div, src/GPU_kernels.cu:1885-2058: product first, then the
+//   division, correctly rounded) with the EPS adjust when asked (kernel_adjust,
+//   :2338-2345); then X's split copies in k_split_factor's layout and its column
+//   sums (matrix_to_row, src/GPU_kernels.cu:871-1066) in FP64: a shuffle tree over
+//   each warp's 8 rows, the 16 warps in order, row blocks in chunks of ECH in block order,
+//   the chunks in order -- fixed orders throughout, so the result does not depend
+//   on scheduling.  It replaces the reference's mul_div + adjust and, for the next
+//   half-iteration, its column sums, in one launch.
+struct FinishArgs {
+    uint32_t O, nsplit, k;
+    int adjust;
+    const float *part;    // [split][O][KP]
+    float *X;
+    const float *accY;    // column sums of Y (KP)
+    float *xhi, *xT;      // X's split copies (SplitLayout of X's rows)
+    __nv_bfloat16 *xBl, *xB, *xBT;
+    uint32_t xnblk32, xnblkbr;
+    double *cs;           // [row block][KP] FP64 column-sum partials, then from row csoff [chunk][KP]
+    uint32_t csoff;
+    float *accX;          // column sums of the new X (KP)
+    uint32_t *tick;       // [chunks + 1] retirement counters (left at 0)
+    const ConvState *st;
+};
+
+template <int KP>
+__global__ void __launch_bounds__(512) k_finish(const FinishArgs a)
+{
+    constexpr int BR = Geo<KP>::BR;
+    constexpr int CPT = KP / 4;          // columns per thread (4 threads per row)
+    constexpr int NW = 16;               // warps
+    if (a.st && *(volatile const uint32_t *)&a.st->converged) return;
+    __shared__ double ws[NW * KP + 512];
+    __shared__ uint32_t eflag;
+    uint32_t const tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
+    uint32_t const row = tid / 4, c0 = (tid % 4) * CPT;
+    uint32_t const oblk = blockIdx.x, nob = gridDim.x;
+    uint32_t const o = oblk * BO + row;
+    bool const in = o < a.O;
+    float x[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) x[c] = 0.0f;
+    if (in) {
+        // Xaux: the split partials in split order, loads issued four splits at a time
+        const float *pr = a.part + (size_t)o * KP + c0;
+        size_t const qs = (size_t)a.O * KP;
+        uint32_t q = 0;
+        for (; q + 4 <= a.nsplit; q += 4) {
+            float4 v[4][CPT / 4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int c = 0; c < CPT / 4; c++) v[j][c] = __ldcg(reinterpret_cast<const float4 *>(pr + (q + j) * qs) + c);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int c = 0; c < CPT / 4; c++) {
+                    x[4 * c] += v[j][c].x;
+                    x[4 * c + 1] += v[j][c].y;
+                    x[4 * c + 2] += v[j][c].z;
+                    x[4 * c + 3] += v[j][c].w;
+                }
+        }
+        for (; q < a.nsplit; q++) {
+#pragma unroll
+            for (int c = 0; c < CPT / 4; c++) {
+                float4 const v = __ldcg(reinterpret_cast<const float4 *>(pr + q * qs) + c);
+                x[4 * c] += v.x;
+                x[4 * c + 1] += v.y;
+                x[4 * c + 2] += v.z;
+                x[4 * c + 3] += v.w;
+            }
+        }
+        float *xr = a.X + (size_t)o * KP + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; c += 4) {
+            float4 const xv = *reinterpret_cast<const float4 *>(xr + c);
+            float const xs[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                uint32_t const cc = c0 + c + i;
+                float v = 0.0f;
+                if (cc < a.k) {
+                    v = __fdiv_rn(xs[i] * x[c + i], __ldg(a.accY + cc));
+                    if (a.adjust) v = fmaxf(v, FLT_MIN);
+                }
+                x[c + i] = v;
+            }
+            *reinterpret_cast<float4 *>(xr + c) = make_float4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+        }
+    }
+    // split copies; rows past the end are zero in the transposed blocks that exist
+    {
+        uint32_t const b32 = o / 32, bbr = o / BR;
+        bool const tin = b32 < a.xnblk32, btin = bbr < a.xnblkbr;
+        float *T32 = a.xT + (size_t)b32 * 2 * KP * 32 + (o % 32);
+        __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + (o % BR);
+#pragma unroll
+        for (int c = 0; c < CPT; c += 4) {
+            float h[4], l[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                h[i] = tf32_rna(x[c + i]);
+                l[i] = x[c + i] - h[i];
+            }
+            if (in) {
+                size_t const e = (size_t)o * KP + c0 + c;
+                *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(bf16x2_rn(l[0], l[1]), bf16x2_rn(l[2], l[3]));
+                *reinterpret_cast<uint2 *>(a.xB + e) = make_uint2(bf16x2_rn(x[c], x[c + 1]), bf16x2_rn(x[c + 2], x[c + 3]));
+            }
+            if (tin) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    T32[(c0 + c + i) * 32] = h[i];
+                    T32[(KP + c0 + c + i) * 32] = l[i];
+                }
+            }
+            if (btin) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) BT[(c0 + c + i) * BR] = __float2bfloat16_rn(x[c + i]);
+            }
+        }
+    }
+    // column sums of this row block: the warp's 8 rows of each column by a shuffle
+    // tree (lanes 4r + g hold row r, column group g), then the 16 warps in order
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        double v = (double)x[c];
+#pragma unroll
+        for (int off = 16; off >= 4; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane < 4) ws[warp * KP + c0 + c] = v;
+    }
+    __syncthreads();
+    if (tid < (uint32_t)KP) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) t += ws[w * KP + tid];
+        a.cs[(size_t)oblk * KP + tid] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    uint32_t const nch = (nob + ECH - 1) / ECH, ch = oblk / ECH;
+    uint32_t const b0 = ch * ECH, bn = min(nob - b0, ECH);
+    if (tid == 0) eflag = (atomicAdd(&a.tick[ch], 1u) == bn - 1) ? 1u : 0u;
+    __syncthreads();
+    if (!eflag) return;
+    // last row block of its chunk: the chunk's partials in block order
+    __threadfence();
+    constexpr int GRP = 512 / KP;
+    uint32_t const g = tid / KP, c = tid % KP;
+    double t = 0.0;
+    for (uint32_t blk = g; blk < bn; blk += GRP) t += __ldcg(a.cs + (size_t)(b0 + blk) * KP + c);
+    ws[NW * KP + tid] = t;
+    __syncthreads();
+    if (tid < (uint32_t)KP) {
+        double u = 0.0;
+        for (int gg = 0; gg < GRP; gg++) u += ws[NW * KP + gg * KP + tid];
+        a.cs[((size_t)a.csoff + ch) * KP + tid] = u;
+    }
+    if (tid == 0) a.tick[ch] = 0u;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) eflag = (atomicAdd(&a.tick[nch], 1u) == nch - 1) ? 1u : 0u;
+    __syncthreads();
+    if (!eflag) return;
+    // last chunk: the chunk sums in order
+    __threadfence();
+    double v = 0.0;
+    for (uint32_t q = g; q < nch; q += GRP) v += __ldcg(a.cs + ((size_t)a.csoff + q) * KP + c);
+    __syncthreads();
+    ws[NW * KP + tid] = v;
+    __syncthreads();
+    if (tid < (uint32_t)KP) {
+        double u = 0.0;
+        for (int gg = 0; gg < GRP; gg++) u += ws[NW * KP + gg * KP + tid];
+        a.accX[tid] = (float)u;
+    }
+    if (tid == 0) a.tick[nch] = 0u;
+}
+
 // Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X and Y
 // producer (TMA), 3 = idle, 4..11 = R warps (V / D, feed MMA2), 12..15 =
 // accumulator warps (sum the per-tile MMA2 results in FP32 registers; split X
@@ -227,7 +412,6 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
 {
     using G = Geo<KP>;
     constexpr int BR = G::BR;
-    constexpr int QW = G::QW;           // tile columns handled by one R warp
     constexpr int NR = G::NR;
     constexpr uint32_t ACC_COLS = G::ACC;
     if (args.st && *(volatile const uint32_t *)&args.st->converged) return;
@@ -282,7 +466,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::VST; s++) {
             mbar_init(&vfull[s], 1);
-            mbar_init(&vempty[s], NR);
+            mbar_init(&vempty[s], NR / 2);   // one team reads each V tile
         }
         for (int s = 0; s < G::YST; s++) {
             mbar_init(&yfull[s], 1);
@@ -290,7 +474,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         }
         for (uint32_t b = 0; b < G::NDB; b++) {
             mbar_init(&dfull[b], 1);
-            mbar_init(&rfull[b], NR);
+            mbar_init(&rfull[b], NR / 2);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&accrdy[b], 1);
@@ -312,8 +496,8 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
     tc_fence_after();
     uint32_t const tmem = *tmem_slot;
 
-    if (T == 0) {
-        // idle
+    if (T == 0 && warp < 4 + NR) {
+        // idle (the accumulator warps write a zero partial)
     } else if (warp == 0) {
         // ------------------------------------------------------------ V producer
         if (lane == 0) {
@@ -473,11 +657,20 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
         }
     } else if (warp >= 4 && warp < 4 + NR) {
         // ------------------------------------------------------------ R warps
+        // Two teams of NR/2 warps take alternate tiles (team 0 even, team 1 odd), so
+        // one team's load latency overlaps the other's arithmetic.  Within a team,
+        // warp (quad, grp) handles TMEM lanes 32 quad .. +31 and CW = BR / GPT tile
+        // columns, in chunks of 16 (one BF16 k-step of MMA2 each).
+        constexpr int TW = NR / 2;                     // warps per team
+        constexpr int GPT = TW / 4;                    // column groups per team
+        constexpr int CW = BR / GPT;                   // tile columns per warp
+        static_assert(CW % 16 == 0, "16-column chunks");
         uint32_t const quad = warp & 3;
-        uint32_t const half = (warp - 4) >> 2;         // column group of this warp
+        uint32_t const jg = (warp - 4) >> 2;
+        uint32_t const team = jg / GPT, grp = jg % GPT;
         uint32_t const row = quad * 32 + lane;        // TMEM lane = output row within the block
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
-        for (uint32_t t = 0; t < T; t++) {
+        for (uint32_t t = team; t < T; t += 2) {
             uint32_t const s = t % G::VST, b = t % G::NDB;
             if (warp == 4 && lane == 0) DBG_TS(4, t);
             DBG_PH(0, t);
@@ -488,71 +681,77 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             DBG_PH(2, t);
             if (warp == 4 && lane == 0) DBG_TS(5, t);
             const unsigned char *sv = sV + s * G::VBYTES;
-            uint32_t const dcol = G::DA0 + b * BR + half * QW;        // this group's columns of D
-            uint32_t const rlcol = G::RL0 + b * (BR / 2) + half * 8;  // and of bf16(Rl)
-            uint32_t d[32];   // D, then the TF32 hi part of R
-            uint32_t v[32];   // V, then the lo part of R
-            tmem_ld16(lane_addr + dcol, d);
-            if (HSIDE) {
-                // V tile [BR rows][128 cols], row-major; this thread's column = row.
-                const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
+#pragma unroll 1
+            for (int ch = 0; ch < CW / 16; ch++) {
+                int const col0 = grp * CW + ch * 16;                          // first tile column of the chunk
+                uint32_t const dcol = G::DA0 + b * BR + col0;                 // its columns of D
+                uint32_t const rlcol = G::RL0 + b * (BR / 2) + (col0 / 16) * 8;  // and of bf16(Rl)
+                uint32_t d[32];   // D, then the TF32 hi part of R
+                uint32_t v[32];   // V, then the lo part of R
+                tmem_ld16(lane_addr + dcol, d);
+                if (HSIDE) {
+                    // V tile [BR rows][128 cols], row-major; this thread's column = row.
+                    const float *vs = reinterpret_cast<const float *>(sv) + col0 * BO + row;
 #pragma unroll
-                for (int c = 0; c < QW; c++) v[c] = __float_as_uint(vs[c * BO]);
-            } else {
-                // V boxes of [128 rows][32 floats], 128B swizzle; this warp's QW columns.
-                int const qb = (half * QW) / 32;
-                int const c0 = ((half * QW) % 32) / 4;      // 16-byte chunk offset within the box
-                const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
+                    for (int c = 0; c < 16; c++) v[c] = __float_as_uint(vs[c * BO]);
+                } else {
+                    // V boxes of [128 rows][32 floats], 128B swizzle.
+                    int const qb = col0 / 32;
+                    int const c0 = (col0 % 32) / 4;      // 16-byte chunk offset within the box
+                    const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
 #pragma unroll
-                for (int c = 0; c < QW / 4; c++) {
-                    uint4 const x = *reinterpret_cast<const uint4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
-                    v[4 * c + 0] = x.x;
-                    v[4 * c + 1] = x.y;
-                    v[4 * c + 2] = x.z;
-                    v[4 * c + 3] = x.w;
+                    for (int c = 0; c < 4; c++) {
+                        uint4 const x = *reinterpret_cast<const uint4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
+                        v[4 * c + 0] = x.x;
+                        v[4 * c + 1] = x.y;
+                        v[4 * c + 2] = x.z;
+                        v[4 * c + 3] = x.w;
+                    }
                 }
-            }
+                if (ch == CW / 16 - 1) {
 #ifdef NMFB_FUSED_DEBUG
-            {   // debug timing only: consume the loaded V values before the next phase mark
-                uint32_t x = 0;
+                    {   // debug timing only: consume the loaded V values before the next phase mark
+                        uint32_t x = 0;
 #pragma unroll
-                for (int c = 0; c < QW; c++) x ^= v[c];
-                asm volatile("" ::"r"(x));
-                if (x == 0x7fffffffu && dts) dts[0] = x;
-            }
+                        for (int c = 0; c < 16; c++) x ^= v[c];
+                        asm volatile("" ::"r"(x));
+                        if (x == 0x7fffffffu && dts) dts[0] = x;
+                    }
 #endif
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
-            DBG_PH(3, t);
-            tmem_wait_ld_dep(d);
-            DBG_PH(4, t);
-            uint32_t pl[8];   // bf16(R lo), packed in column pairs
-#pragma unroll
-            for (int c = 0; c < QW; c++) {
-                // R = V / WH as V * (1/WH): the approximate reciprocal (<= 1 ulp) runs at
-                // full rate, the fast-division intrinsic at a third of it.  min(., FLT_MAX)
-                // keeps the zero-filled edges (V = 0, WH = 0) at 0 instead of 0 * inf.
-                float const vv = __uint_as_float(v[c]);
-                float const wh = __uint_as_float(d[c]);
-                float const r = vv * fminf(rcp_approx(wh), FLT_MAX);
-                float const h = tf32_rna(r);
-#ifdef NMFB_FUSED_DEBUG
-                if (args.dbg && blockIdx.x == 0 && t == 0) {
-                    args.dbg[row * 64 + half * QW + c] = wh;
-                    args.dbg[BO * 64 + row * 64 + half * QW + c] = vv;
-                    args.dbg[2 * BO * 64 + row * 64 + half * QW + c] = h;
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&vempty[s]);      // V stage consumed (values are in registers)
+                    DBG_PH(3, t);
                 }
-#endif
-                d[c] = __float_as_uint(h);
-                v[c] = __float_as_uint(r - h);
-            }
-            if (NTERMS == 3) {
+                tmem_wait_ld_dep(d);
+                if (ch == CW / 16 - 1) DBG_PH(4, t);
+                uint32_t pl[8];   // bf16(R lo), packed in column pairs
 #pragma unroll
-                for (int j = 0; j < QW / 2; j++) pl[j] = bf16x2_rn(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
+                for (int c = 0; c < 16; c++) {
+                    // R = V / WH as V * (1/WH): the approximate reciprocal (<= 1 ulp) runs at
+                    // full rate, the fast-division intrinsic at a third of it.  min(., FLT_MAX)
+                    // keeps the zero-filled edges (V = 0, WH = 0) at 0 instead of 0 * inf.
+                    float const vv = __uint_as_float(v[c]);
+                    float const wh = __uint_as_float(d[c]);
+                    float const r = vv * fminf(rcp_approx(wh), FLT_MAX);
+                    float const h = tf32_rna(r);
+#ifdef NMFB_FUSED_DEBUG
+                    if (args.dbg && blockIdx.x == 0 && t == 0) {
+                        args.dbg[row * 64 + col0 + c] = wh;
+                        args.dbg[BO * 64 + row * 64 + col0 + c] = vv;
+                        args.dbg[2 * BO * 64 + row * 64 + col0 + c] = h;
+                    }
+#endif
+                    d[c] = __float_as_uint(h);
+                    v[c] = __float_as_uint(r - h);
+                }
+                if (NTERMS == 3) {
+#pragma unroll
+                    for (int j = 0; j < 8; j++) pl[j] = bf16x2_rn(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
+                }
+                if (ch == CW / 16 - 1) DBG_PH(5, t);
+                tmem_st16(lane_addr + dcol, d);
+                if (NTERMS == 3) tmem_st8(lane_addr + rlcol, pl);
             }
-            DBG_PH(5, t);
-            tmem_st16(lane_addr + dcol, d);
-            if (NTERMS == 3) tmem_st8(lane_addr + rlcol, pl);
             tmem_wait_st();
             DBG_PH(6, t);
             tc_fence_before();
@@ -575,7 +774,7 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
 #pragma unroll
         for (int c = 0; c < KP; c++) sum[c] = 0.0f;
         bool ok = true;
-        {   // this thread's row of X as TF32 hi and bf16(hi) | bf16(lo), into TMEM lanes = rows
+        if (T > 0) {   // this thread's row of X as TF32 hi and bf16(hi) | bf16(lo), into TMEM lanes = rows
             uint32_t const o = o0 + row;
             const float *xr = args.X + (size_t)o * KP;
 #pragma unroll
@@ -635,25 +834,19 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             if (lane == 0 && dts && blockIdx.x == 0 && t < 64) dts[1024 + (warp - 4 - NR) * 64 + t] = globaltimer() - ts0;
 #endif
         }
+#ifdef NMFB_FUSED_DEBUG
+        if (ok && args.dbg && blockIdx.x == 0)
+            for (int c = 0; c < KP; c++) args.dbg[3 * BO * 64 + row * KP + c] = sum[c];
+#endif
+        // this split's partial (zero for an idle split); k_finish sums the splits
         if (ok) {
             uint32_t const o = o0 + row;
-#ifdef NMFB_FUSED_DEBUG
-            if (args.dbg && blockIdx.x == 0)
-                for (int c = 0; c < KP; c++) args.dbg[3 * BO * 64 + row * KP + c] = sum[c];
-#endif
             if (o < args.O) {
                 float *dst = args.part + ((size_t)split * args.O + o) * KP;
 #pragma unroll
                 for (int c = 0; c < KP; c += 4)
                     *reinterpret_cast<float4 *>(dst + c) = make_float4(sum[c], sum[c + 1], sum[c + 2], sum[c + 3]);
             }
-        }
-    }
-    if (T == 0 && warp >= 4 + NR) {
-        uint32_t const o = o0 + (warp & 3) * 32 + lane;
-        if (o < args.O) {
-            float *dst = args.part + ((size_t)split * args.O + o) * KP;
-            for (int c = 0; c < KP; c++) dst[c] = 0.0f;
         }
     }
     tc_fence_before();
@@ -720,13 +913,16 @@ struct FusedPlan {
     FusedMaps mapsH, mapsW;  // update_H (HSIDE) and update_W
     uint32_t *dErr;
     float *dSplitW, *dSplitH;  // split copies of W and of H (k_split_factor, SplitLayout)
+    double *dCs;               // [row blocks + chunks][kp] column-sum partials of k_finish
+    uint32_t *dTick;           // [chunks + 1] retirement counters of k_finish
+    uint32_t nticks, csoff;
 #ifdef NMFB_FUSED_DEBUG
     float *dDbg;
 #endif
 };
 
 template <bool HSIDE, int KP, int NTERMS>
-int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
+int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
 {
     using G = Geo<KP>;
     constexpr int BR = G::BR;
@@ -774,47 +970,82 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps)
     kern<<<oblocks * nsplit, G::NTHR, G::SMEM, ctx->stream>>>(maps, args);
     NMFB_LAUNCH_CHECK(ctx);
     if ((rc = nmfb_prof_end(ctx, main))) return rc;
+
+    FinishArgs fa;
+    float *xsp = HSIDE ? plan->dSplitH : plan->dSplitW;
+    SplitLayout const L(O, KP);
+    fa.O = O;
+    fa.nsplit = nsplit;
+    fa.k = ctx->k;
+    fa.adjust = adjust;
+    fa.part = ctx->dPart;
+    fa.X = HSIDE ? ctx->dH : ctx->dW;
+    fa.accY = HSIDE ? ctx->dAccW : ctx->dAccH;
+    fa.xhi = xsp;
+    fa.xT = xsp + L.t;
+    fa.xBl = reinterpret_cast<__nv_bfloat16 *>(xsp + L.bl);
+    fa.xB = reinterpret_cast<__nv_bfloat16 *>(xsp + L.b);
+    fa.xBT = reinterpret_cast<__nv_bfloat16 *>(xsp + L.bt);
+    fa.xnblk32 = L.nblk32;
+    fa.xnblkbr = L.nblkbr;
+    fa.cs = plan->dCs;
+    fa.csoff = plan->csoff;
+    fa.accX = HSIDE ? ctx->dAccH : ctx->dAccW;
+    fa.tick = plan->dTick;
+    fa.st = ctx->dState;
+    if (oblocks > plan->csoff || (oblocks + ECH - 1) / ECH + 1 > plan->nticks)
+        return nmfb_fail(ctx, NMFB_EINVAL, "fused: column-sum buffers too small");
+    k_finish<KP><<<oblocks, 512, 0, ctx->stream>>>(fa);
+    NMFB_LAUNCH_CHECK(ctx);
     return (int)nsplit;
 }
 
 template <bool HSIDE>
-int dispatch(nmfb_ctx *ctx, const FusedMaps &maps)
+int dispatch(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
 {
     bool const x3 = ctx->arm == NMFB_ARM_FUSED;
     switch (ctx->kp) {
-    case 16: return x3 ? launch_fused<HSIDE, 16, 3>(ctx, maps) : launch_fused<HSIDE, 16, 1>(ctx, maps);
-    case 32: return x3 ? launch_fused<HSIDE, 32, 3>(ctx, maps) : launch_fused<HSIDE, 32, 1>(ctx, maps);
-    case 64: return x3 ? launch_fused<HSIDE, 64, 3>(ctx, maps) : launch_fused<HSIDE, 64, 1>(ctx, maps);
+    case 16: return x3 ? launch_fused<HSIDE, 16, 3>(ctx, maps, adjust) : launch_fused<HSIDE, 16, 1>(ctx, maps, adjust);
+    case 32: return x3 ? launch_fused<HSIDE, 32, 3>(ctx, maps, adjust) : launch_fused<HSIDE, 32, 1>(ctx, maps, adjust);
+    case 64: return x3 ? launch_fused<HSIDE, 64, 3>(ctx, maps, adjust) : launch_fused<HSIDE, 64, 1>(ctx, maps, adjust);
     default: return nmfb_fail(ctx, NMFB_EINVAL, "fused arm: unsupported padded rank %u", ctx->kp);
     }
 }
 
+// Split copies and column sums of a factor, for a half-iteration that reads
+// it as Y when the previous half-iteration's epilogue did not produce them.
+int prepare_factor(nmfb_ctx *ctx, bool w)
+{
+    FusedPlan *plan = (FusedPlan *)ctx->tmaps;
+    const float *F = w ? ctx->dW : ctx->dH;
+    uint32_t const rows = w ? ctx->n : ctx->m;
+    int rc = nmfb_colsum(ctx, F, rows, w ? ctx->dAccW : ctx->dAccH, w ? 0 : 1);
+    if (rc) return rc;
+    float *sp = w ? plan->dSplitW : plan->dSplitH;
+    SplitLayout const L(rows, ctx->kp);
+    k_split_factor<<<L.nblkbr, 256, 0, ctx->stream>>>(F, rows, ctx->kp, L.br, sp, sp + L.t,
+                                                     reinterpret_cast<__nv_bfloat16 *>(sp + L.bl),
+                                                     reinterpret_cast<__nv_bfloat16 *>(sp + L.b),
+                                                     reinterpret_cast<__nv_bfloat16 *>(sp + L.bt), ctx->dState);
+    NMFB_LAUNCH_CHECK(ctx);
+    ctx->fz_ok[w ? 0 : 1] = 1;
+    return NMFB_OK;
+}
+
+// One half-iteration: a single launch when the other factor's split copies and
+// column sums are current (the previous half-iteration's epilogue wrote them).
 int fused_half(nmfb_ctx *ctx, bool is_H, int adjust)
 {
     FusedPlan *plan = (FusedPlan *)ctx->tmaps;
     if (!plan) return nmfb_fail(ctx, NMFB_ESTATE, "fused arm not prepared");
-    float *X = is_H ? ctx->dH : ctx->dW;
-    const float *Y = is_H ? ctx->dW : ctx->dH;
-    uint32_t const xrows = is_H ? ctx->m : ctx->n;
-    uint32_t const yrows = is_H ? ctx->n : ctx->m;
-    float *acc = is_H ? ctx->dAccW : ctx->dAccH;
     int const whole = is_H ? 2 : 3;
     int rc = nmfb_prof_begin(ctx, whole);
     if (rc) return rc;
-    if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
-    {
-        float *sp = is_H ? plan->dSplitW : plan->dSplitH;
-        SplitLayout const L(yrows, ctx->kp);
-        k_split_factor<<<L.nblkbr, 256, 0, ctx->stream>>>(Y, yrows, ctx->kp, L.br, sp, sp + L.t,
-                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.bl),
-                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.b),
-                                                         reinterpret_cast<__nv_bfloat16 *>(sp + L.bt), ctx->dState);
-        NMFB_LAUNCH_CHECK(ctx);
-    }
-    int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH) : dispatch<false>(ctx, plan->mapsW);
+    bool const yw = is_H;   // Y = W for update_H
+    if (!ctx->fz_ok[yw ? 0 : 1] && (rc = prepare_factor(ctx, yw))) return rc;
+    int const nsplit = is_H ? dispatch<true>(ctx, plan->mapsH, adjust) : dispatch<false>(ctx, plan->mapsW, adjust);
     if (nsplit < 0) return nsplit;
-    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust);
-    if (rc) return rc;
+    ctx->fz_ok[is_H ? 1 : 0] = 1;
     return nmfb_prof_end(ctx, whole);
 }
 
@@ -860,7 +1091,14 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     uint32_t const br = LW.br;
     e = nmfb_malloc(ctx, (void **)&plan->dSplitW, LW.floats * sizeof(float));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, LH.floats * sizeof(float));
+    uint32_t const maxblk = ((ctx->n > ctx->m ? ctx->n : ctx->m) + BO - 1) / BO;
+    plan->csoff = maxblk;
+    plan->nticks = (maxblk + ECH - 1) / ECH + 1;
+    if (e == cudaSuccess)
+        e = nmfb_malloc(ctx, (void **)&plan->dCs, (size_t)(maxblk + (maxblk + ECH - 1) / ECH) * kp * sizeof(double));
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dTick, plan->nticks * sizeof(uint32_t));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused split buffers: %s", cudaGetErrorString(e));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dTick, 0, plan->nticks * sizeof(uint32_t), ctx->own_stream));
     // Maps over one factor's split copies: Y (the other factor, `rows` rows).
     auto const y_maps = [&](FusedMaps &mp, const float *sp, const SplitLayout &L, uint32_t rows) -> int {
         int r;
@@ -892,12 +1130,22 @@ int nmfb_fused_release(nmfb_ctx *ctx)
     if (plan->dErr) nmfb_free(ctx, plan->dErr);
     if (plan->dSplitW) nmfb_free(ctx, plan->dSplitW);
     if (plan->dSplitH) nmfb_free(ctx, plan->dSplitH);
+    if (plan->dCs) nmfb_free(ctx, plan->dCs);
+    if (plan->dTick) nmfb_free(ctx, plan->dTick);
     free(plan);
     ctx->tmaps = nullptr;
     return NMFB_OK;
 }
 
 int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust) { return fused_half(ctx, true, adjust); }
+
+// Makes W's split copies and column sums current (before a test block is
+// replayed as a graph, which holds no preparation launch).
+int nmfb_fused_ready_W(nmfb_ctx *ctx)
+{
+    if (!ctx->tmaps || ctx->fz_ok[0]) return NMFB_OK;
+    return prepare_factor(ctx, true);
+}
 int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust) { return fused_half(ctx, false, adjust); }
 
 uint32_t *nmfb_fused_err_word(nmfb_ctx *ctx)
@@ -917,7 +1165,10 @@ int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code)
     NMFB_CUDA_TRY(ctx, cudaMemcpyAsync(code, plan->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (*code) {
+        // an aborted launch may have left retirement counters and factor copies behind
         NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dErr, 0, sizeof(uint32_t), ctx->stream));
+        NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dTick, 0, plan->nticks * sizeof(uint32_t), ctx->stream));
+        ctx->fz_ok[0] = ctx->fz_ok[1] = 0;
         NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     }
     return NMFB_OK;

@@ -439,6 +439,7 @@ int nmfb_update_H(nmfb_ctx *ctx)
 {
     int rc = ready(ctx);
     if (rc) return rc;
+    ctx->fz_ok[0] = ctx->fz_ok[1] = 0;   // the caller may have changed W or H since
     return do_update_H(ctx, 0);
 }
 
@@ -446,6 +447,7 @@ int nmfb_update_W(nmfb_ctx *ctx)
 {
     int rc = ready(ctx);
     if (rc) return rc;
+    ctx->fz_ok[0] = ctx->fz_ok[1] = 0;
     return do_update_W(ctx, 0);
 }
 
@@ -479,6 +481,7 @@ static int enqueue_block(nmfb_ctx *ctx, uint32_t J)
         if (!rc) rc = do_update_W(ctx, i + 1 == J);
     }
     if (!rc) rc = nmfb_classify_and_test(ctx, J);
+    ctx->fz_ok[1] = 0;   // the test's EPS adjust rewrote H
     return rc;
 }
 
@@ -488,6 +491,9 @@ static int launch_block(nmfb_ctx *ctx, uint32_t J)
 {
     static int const use_graphs = getenv("NMFB_NO_GRAPHS") == nullptr;
     if (!use_graphs || ctx->prof_on || ctx->splan) return enqueue_block(ctx, J);
+    // the graph holds no preparation launch: make W's split copies current first
+    int const rc0 = (ctx->arm == NMFB_ARM_FUSED || ctx->arm == NMFB_ARM_FUSED_TF32) ? nmfb_fused_ready_W(ctx) : NMFB_OK;
+    if (rc0) return rc0;
     if (!ctx->blk_exec || ctx->blk_J != J || ctx->blk_arm != ctx->arm || ctx->blk_stream != ctx->stream ||
         ctx->blk_wait != ctx->wait_ns) {
         if (ctx->blk_exec) {
@@ -518,6 +524,8 @@ static int launch_block(nmfb_ctx *ctx, uint32_t J)
     }
     NMFB_CUDA_TRY(ctx, cudaGraphLaunch(ctx->blk_exec, ctx->stream));
     ctx->launches += ctx->blk_kernels;
+    ctx->fz_ok[0] = 1;   // the block ends with update_W's epilogue and the test's adjust of H
+    ctx->fz_ok[1] = 0;
     return NMFB_OK;
 }
 
@@ -529,6 +537,7 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     if (n_iters == 0 || niter_test_conv == 0 || stop_threshold == 0)
         return nmfb_fail(ctx, NMFB_EINVAL, "nIters, niter_test_conv and stop_threshold must be positive");
     if ((rc = nmfb_reset_conv(ctx, stop_threshold))) return rc;
+    ctx->fz_ok[0] = ctx->fz_ok[1] = 0;
     uint32_t const niter_conv = n_iters / niter_test_conv;
     uint32_t const niter_rem = n_iters % niter_test_conv;
     // Test blocks are queued in batches; the host looks at the device state of
@@ -585,6 +594,7 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     }
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
+    ctx->fz_ok[0] = ctx->fz_ok[1] = 0;
     if (rc) return rc;
     {
         uint32_t code = 0;

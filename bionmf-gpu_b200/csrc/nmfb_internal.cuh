@@ -56,6 +56,11 @@ struct nmfb_ctx {
     nmfb::ConvState *dState;
     nmfb::ConvState *hState;  // pinned host mirror
 
+    // Fused arm: the split copies and column sums of W ([0]) and of H ([1]) match
+    // the factor (written by the previous half-iteration's epilogue).  Trusted
+    // only inside one nmfb_run or step call; every entry point starts from 0.
+    int fz_ok[2];
+
     uint64_t launches;
     unsigned long long wait_ns;  // bounded-wait limit of the fused kernels (0: the 1 s default)
     // CUDA graph of one convergence-test block (nmfb_run): replayed instead of
@@ -143,6 +148,7 @@ int nmfb_fused_release(nmfb_ctx *ctx);
 int nmfb_fused_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_fused_update_W(nmfb_ctx *ctx, int adjust);
 int nmfb_fused_error(nmfb_ctx *ctx, uint32_t *code);
+int nmfb_fused_ready_W(nmfb_ctx *ctx);
 uint32_t *nmfb_fused_err_word(nmfb_ctx *ctx);
 
 // ---- kernels_bf16.cu ------------------------------------------------------

@@ -40,7 +40,8 @@ extern "C" {
 
 /* Update kernels ("arms").  All arms run the same method; they differ only
  * in how the two n x m x k contractions of a half-iteration are evaluated. */
-#define NMFB_ARM_FUSED 0  /* fused half-iteration, tcgen05 3xTF32 (FP32-accurate) */
+#define NMFB_ARM_FUSED 0  /* fused half-iteration (one launch): TF32 hi x (hi + lo) products plus the
+                           * lo x y term as a BF16 product, FP32 accumulation (FP32-accurate, ~2^-20 per product) */
 #define NMFB_ARM_PLAIN 1  /* unfused FP32 SIMT kernels mirroring the reference's 5 steps */
 #define NMFB_ARM_FUSED_TF32 2 /* fused, 1xTF32 denominator (reduced precision) */
 #define NMFB_ARM_BF16 3       /* fused, BF16 operands, FP32 accumulation (reduced precision) */

@@ -125,6 +125,33 @@ def test_rank_sweep_recovers_planted_rank(pkg, synth):
     assert res.device_ms > 0
 
 
+def test_autotuner_tiles_keep_the_method(pkg, oracle, synth):
+    # the tile autotuner picks (wt, jt) per rank from its candidates, caches the
+    # choice, and a batch run with the chosen tiles matches the FP64 oracle
+    import nmf_b200.sweep as sweep
+
+    V, _ = synth.config_d(4)
+    n, m = V.shape
+    tiles = sweep.autotune(V, [3, 5], iters=10)
+    assert set(tiles) == {3, 5}
+    for wt, jt in tiles.values():
+        assert wt in sweep.WT_CANDIDATES and jt in sweep.JT_CANDIDATES
+    assert sweep.autotune(V, [5]) == {5: tiles[5]}       # cached per (k, m, n) bucket
+    ranks = [3, 3, 5, 5]
+    seeds = [1, 2, 1, 2]
+    with pkg.Batch(n, m, ranks) as b:
+        b.set_V(V)
+        for p, k in enumerate(ranks):
+            b.set_tiles(p, *tiles[k])
+        b.init_random(seeds)
+        it, conv = b.run(30, 10, 10 ** 9)
+        assert (it == 30).all()
+        for p, (k, sd) in enumerate(zip(ranks, seeds)):
+            W0, H0 = oracle.init_random(sd, n, m, k)
+            Wr, Hr, _, _ = oracle.nmf(V, W0, H0, 30, 10, 10 ** 9, prec="f64")
+            assert maxnorm_rel(b.W(p), Wr) < 1e-4 and maxnorm_rel(b.H(p), Hr) < 1e-4
+
+
 @pytest.mark.parametrize("ctas", [1, 2, 4, 8])
 def test_cluster_split_problems(pkg, oracle, synth, ctas):
     # Each problem on a cluster of `ctas` CTAs (rows of W split, partial sums
