@@ -460,11 +460,12 @@ def sweep_rates(dev, steps=2, warmup=1, seq_sample=2, flush=None):
             "l2": "256 MB buffer written before every sweep"}
 
 
-def stream_rates(dev, iters=3):
+def stream_rates(dev, iters=10):
     """Blockwise mode on the S32 workload: iterations/s with V read from
-    page-locked host memory every half-iteration, the achieved host-to-device
-    rate (2 n m 4 bytes per iteration) and the measured copy peak of the link
-    (one 1 GiB pinned host-to-device copy)."""
+    page-locked host memory, one convergence-test block of `iters` iterations
+    (update_W's pass over V also forms the next update_H's sum, except after
+    the block's last update_W: iters + 1 passes), the achieved host-to-device
+    rate and the measured copy peak of the link (one 1 GiB pinned copy)."""
     import torch
     pkg = _import_package()
     n, m, k, _, desc = WORKLOADS["S32"]
@@ -499,10 +500,12 @@ def stream_rates(dev, iters=3):
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1)
     rate = iters / (ms / 1e3)
-    h2d = 2.0 * n * m * 4 * iters / (ms / 1e3) / 1e9
+    passes = iters + 1
+    h2d = float(passes) * n * m * 4 / (ms / 1e3) / 1e9
     return {"workload": desc, "value": rate, "unit": "iters/s", "h2d_gbs": h2d, "h2d_peak_gbs": peak,
-            "frac_of_link": h2d / peak, "bytes_per_iteration": 2 * n * m * 4,
-            "cbig_s_per_iter_at_this_rate": 2.0 * 250000 * 200000 * 4 / (h2d * 1e9),
+            "frac_of_link": h2d / peak, "passes_per_iteration": passes / iters,
+            "bytes_per_iteration": passes / iters * n * m * 4,
+            "cbig_s_per_iter_at_this_rate": passes / iters * 250000 * 200000 * 4 / (h2d * 1e9),
             "note": "250000x200000 (200 GB) is larger than this host's 196 GB of RAM; the blockwise path is "
                     "link-bound and linear in bytes, so its per-iteration time is extrapolated"}
 

@@ -547,6 +547,7 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     cudaEvent_t ev[2];
     NMFB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
     NMFB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    ctx->in_run = 1;
     int stopped = 0;
     uint32_t b = 0, q = 0;
     while (b < niter_conv && !stopped) {
@@ -595,6 +596,8 @@ int nmfb_run(nmfb_ctx *ctx, uint32_t n_iters, uint32_t niter_test_conv, uint32_t
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
     ctx->fz_ok[0] = ctx->fz_ok[1] = 0;
+    ctx->in_run = 0;
+    if (ctx->splan) nmfb_stream_end_run(ctx);
     if (rc) return rc;
     {
         uint32_t code = 0;

@@ -60,6 +60,10 @@ struct nmfb_ctx {
     // the factor (written by the previous half-iteration's epilogue).  Trusted
     // only inside one nmfb_run or step call; every entry point starts from 0.
     int fz_ok[2];
+    // Inside nmfb_run: the blockwise mode may fold the next update_H's pass over
+    // V into update_W's pass (the factors change only through the run's own
+    // updates there).
+    int in_run;
 
     uint64_t launches;
     unsigned long long wait_ns;  // bounded-wait limit of the fused kernels (0: the 1 s default)
@@ -141,6 +145,7 @@ int nmfb_stream_set_V(nmfb_ctx *ctx, const float *V, size_t ldv);
 int nmfb_stream_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_stream_update_W(nmfb_ctx *ctx, int adjust);
 int nmfb_stream_objectives(nmfb_ctx *ctx, double out[3]);
+void nmfb_stream_end_run(nmfb_ctx *ctx);
 
 // ---- kernels_fused.cu -----------------------------------------------------
 int nmfb_fused_prepare(nmfb_ctx *ctx);

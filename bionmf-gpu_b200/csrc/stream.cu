@@ -8,10 +8,7 @@
 // device block buffers (double buffering): the copy of block b+1 overlaps the
 // kernels of block b, ordered by events (copied[slot] before the kernels that
 // read the slot, consumed[slot] before the next copy into it).  W, H and all
-// other state stay resident.  Each half-iteration reads V once, so an
-// iteration moves 2 n m 4 bytes over PCIe / C2C: the schedule keeps the
-// reference's update order (all of update_H, then all of update_W), which a
-// single pass over V cannot do.
+// other state stay resident.
 //
 //   update_H: acc = colsum(W); for every row block b:
 //               WH_b = W_b H^T, Q_b = V_b ./ WH_b, Aux += Q_b^T W_b
@@ -19,6 +16,16 @@
 //             the result does not depend on timing); H = H .* Aux ./ acc.
 //   update_W: acc = colsum(H); for every row block b (independent rows):
 //               WH_b = W_b H^T, Q_b = V_b ./ WH_b, W_b = W_b .* (Q_b H) ./ acc.
+//
+// Single pass over V per iteration: inside nmfb_run, an update_W that is not
+// the last of a convergence-test block also computes, while V_b is on the
+// device, the next update_H's block term with the block's new W rows and the
+// unchanged H (WH'_b = W'_b H^T, Q'_b = V_b ./ WH'_b, Aux += Q'_b^T W'_b); the
+// next update_H then only applies H = H .* Aux ./ colsum(W').  The kernels,
+// operands and block order are those of the separate pass, so the results are
+// identical; V crosses the link once per iteration instead of twice (11 passes
+// per test block of 10 iterations: the block's first update_H still reads V,
+// because the test's EPS adjust rewrites H after the block's last update_W).
 // The kernels are the plain FP32 arm's (kernels_plain.cu) on row blocks: the
 // path is bound by the host link, two orders of magnitude below HBM.
 #include "nmfb_internal.cuh"
@@ -38,6 +45,7 @@ struct StreamPlan {
     cudaStream_t cs;        // copy stream
     cudaEvent_t copied[2], consumed[2];
     int used[2];
+    int haux_ready;         // dAux holds the next update_H's sum (from update_W's pass)
 };
 
 __global__ void k_accum(float *__restrict__ aux, const float *__restrict__ part, uint32_t nsplit, size_t stride,
@@ -184,6 +192,12 @@ int nmfb_stream_update_H(nmfb_ctx *ctx, int adjust)
     if (rc) return rc;
     if ((rc = nmfb_colsum(ctx, ctx->dW, ctx->n, ctx->dAccW, 0))) return rc;
     size_t const total = (size_t)ctx->m * ctx->kp;
+    if (p->haux_ready) {
+        // the sum was formed during the previous update_W's pass over V
+        p->haux_ready = 0;
+        if ((rc = nmfb_muldiv(ctx, ctx->dH, ctx->m, p->dAux, 1, total, ctx->dAccW, adjust))) return rc;
+        return nmfb_prof_end(ctx, 2);
+    }
     unsigned grid = (unsigned)((total + 255) / 256);
     if (grid > 8u * (unsigned)ctx->sm_count) grid = 8u * (unsigned)ctx->sm_count;
     rc = for_blocks(ctx, p, [&](uint32_t b, uint32_t i0, uint32_t nb, const float *Vb) -> int {
@@ -208,17 +222,39 @@ int nmfb_stream_update_W(nmfb_ctx *ctx, int adjust)
     int rc = nmfb_prof_begin(ctx, 3);
     if (rc) return rc;
     if ((rc = nmfb_colsum(ctx, ctx->dH, ctx->m, ctx->dAccH, 1))) return rc;
-    rc = for_blocks(ctx, p, [&](uint32_t, uint32_t i0, uint32_t nb, const float *Vb) -> int {
+    // fold the next update_H's pass into this one (see the file comment)
+    bool const fold = ctx->in_run && !adjust;
+    size_t const total = (size_t)ctx->m * ctx->kp;
+    unsigned grid = (unsigned)((total + 255) / 256);
+    if (grid > 8u * (unsigned)ctx->sm_count) grid = 8u * (unsigned)ctx->sm_count;
+    p->haux_ready = 0;
+    rc = for_blocks(ctx, p, [&](uint32_t b, uint32_t i0, uint32_t nb, const float *Vb) -> int {
         float *Wb = ctx->dW + (size_t)i0 * ctx->kp;
         int r = nmfb_plain_wh(ctx, Wb, nb, p->dWHb);
         if (!r) r = nmfb_plain_div(ctx, Vb, p->dWHb, nb);
         uint32_t ns = 0;
         if (!r) r = nmfb_plain_red(ctx, p->dWHb, 0, ctx->dH, nb, ctx->m, &ns);
         if (!r) r = nmfb_muldiv(ctx, Wb, nb, ctx->dPart, ns, (size_t)nb * ctx->kp, ctx->dAccH, adjust);
-        return r;
+        if (r || !fold) return r;
+        // next update_H's term of this block, with the new W rows
+        r = nmfb_plain_wh(ctx, Wb, nb, p->dWHb);
+        if (!r) r = nmfb_plain_div(ctx, Vb, p->dWHb, nb);
+        if (!r) r = nmfb_plain_red(ctx, p->dWHb, 1, Wb, ctx->m, nb, &ns);
+        if (r) return r;
+        k_accum<<<grid, 256, 0, ctx->stream>>>(p->dAux, ctx->dPart, ns, total, total, b == 0, ctx->dState);
+        NMFB_LAUNCH_CHECK(ctx);
+        return NMFB_OK;
     });
     if (rc) return rc;
+    p->haux_ready = fold ? 1 : 0;
     return nmfb_prof_end(ctx, 3);
+}
+
+// End of nmfb_run: a sum formed by the run's last update_W is not used.
+void nmfb_stream_end_run(nmfb_ctx *ctx)
+{
+    StreamPlan *p = plan_of(ctx);
+    if (p) p->haux_ready = 0;
 }
 
 int nmfb_stream_objectives(nmfb_ctx *ctx, double out[3])

@@ -5,7 +5,9 @@ Tolerances: against the FP64 oracle as for the resident arms (1e-4 after a
 fixed iteration count; identical iteration count and classification at
 convergence); against the resident plain FP32 arm 1e-5 (only the order of the
 FP32 partial sums differs); the block-wise FP64 objectives within 1e-9 relative
-of the oracle's on the same factors.
+of the oracle's on the same factors.  Inside a run, update_W's pass over V also
+forms the next update_H's sum (one pass per iteration); the same run done as
+single update calls, one pass per half-iteration, must give identical factors.
 """
 from __future__ import annotations
 
@@ -75,3 +77,24 @@ def test_streamed_single_updates_and_restrictions(pkg, oracle, synth):
         e.set_WH(W0, H0)
         e.update_H()
         assert maxnorm_rel(e.H, oracle.update_H(V2, W0, H0, prec="f64")) < 1e-5
+
+
+def test_single_pass_equals_separate_passes(pkg, oracle, synth):
+    # nmfb_run folds update_H's pass into the previous update_W's pass (except
+    # after a test block's last update_W, whose EPS adjust of H follows); the
+    # same updates as single calls (two passes per iteration) give the same
+    # factors bit for bit: same kernels, same operands, same block order
+    V, _ = synth.expression_like(900, 130, 6, seed=12, zero_frac=0.02)
+    n, m = V.shape
+    W0, H0 = oracle.init_random(5, n, m, 6)
+    with pkg.NMF(n, m, 6, stream_rows=128) as a, pkg.NMF(n, m, 6, stream_rows=128) as b:
+        for e in (a, b):
+            e.set_V(V)
+            e.set_WH(W0, H0)
+        assert a.run(7, 10, 1000) == (7, False)       # no test block: no adjust, every W pass folded
+        for _ in range(7):
+            b.update_H()
+            b.update_W()
+        assert np.array_equal(a.W, b.W) and np.array_equal(a.H, b.H)
+        Wr, Hr, _, _ = oracle.nmf(V, W0, H0, 7, 10, 1000, prec="f64")
+        assert maxnorm_rel(a.W, Wr) < 1e-4 and maxnorm_rel(a.H, Hr) < 1e-4
