@@ -86,6 +86,15 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def arm_precision():
+    """Measured error of every fused arm against FP64 (6000 x 500 submatrix), committed with the profiles."""
+    p = os.path.join(ROOT, "profiles", "arm_precision.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
 def ncu_traffic(kernel_key: str):
     """DRAM bytes per launch of the dominant kernel from a committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -767,6 +776,15 @@ def run_engine_arm(a, rank, world, local_rank):
         extras["plain_arm"]["fused_speedup"] = value / extras["plain_arm"]["value"]
         extras["arms"] = {arm: guarded(other_arm_rate, a, pkg, V, dev, stream, n, m, k, hbm, arm)
                           for arm in ("bf16x3", "split_bf16", "bf16", "fused_tf32")}
+        # each arm's error against FP64 on the 6000 x 500 submatrix, as measured by
+        # the committed parity test's case (profiles/arm_precision.json)
+        prec = arm_precision()
+        if prec:
+            extras["precision_vs_fp64"] = {"fused": prec.get(f"k{k}:fused"), "source": "profiles/arm_precision.json"}
+            for arm, entry in extras["arms"].items():
+                if isinstance(entry, dict) and f"k{k}:{arm}" in prec:
+                    entry["precision_vs_fp64"] = prec[f"k{k}:{arm}"]
+                    entry["speedup_vs_fp32_arm"] = entry.get("value", 0.0) / value
         del V
         torch.cuda.empty_cache()
         extras["workloads"] = {wl: guarded(workload_rate, a, pkg, dev, wl, hbm) for wl in ("C64", "B16")}

@@ -7,8 +7,9 @@
 //   D   = X Y^T                      (MMA1, TMEM, FP32 accumulate)
 //   R   = V / D                      (R warps, FP32 registers)
 //   Acc = R Y                        (MMA2, TMEM, FP32 accumulate)
-// and Acc is summed per tile into FP32 registers; k_factor then applies
-// X = X .* (sum of splits) ./ colsum(Y).  What changes is the operand type of
+// and Acc is summed per tile into FP32 registers; k_finish (finish.cuh) then
+// applies X = X .* (sum of splits) ./ colsum(Y) and writes X's BF16 copies and
+// column sums for the next half-iteration.  What changes is the operand type of
 // the two contractions (tcgen05.mma kind::f16, BF16 A and B, K = 16 per
 // instruction, FP32 accumulation):
 //   NMFB_ARM_BF16       : X, Y, R rounded to BF16 (one product each);
@@ -24,10 +25,12 @@
 // 8-bit exponent, so a per-column rescaling of the factors would change no
 // rounding error and is not applied.
 //
-// All operands reach shared memory by TMA in the layout the MMA reads:
-// k_split_bf16 writes BF16 hi / lo copies of X and Y (rows x KP, K-major) and,
-// for Y, per 64-row block the transposed hi block followed by the transposed
-// lo block (64 rows of Y -> 2 KP rows of 64 values) that MMA2 reads K-major.
+// All operands reach shared memory by TMA in the layout the MMA reads: BF16
+// hi / lo copies of X and Y (rows x KP, K-major) and, per 64-row block, the
+// transposed hi block followed by the transposed lo block (64 rows -> 2 KP rows
+// of 64 values) that MMA2 reads K-major -- written by k_finish when the factor
+// is updated, or by k_split_bf16 when it is not current (start of a run, after
+// the test's EPS adjust of H).  The R warps work in two teams on alternate tiles.
 // R goes to shared memory (128B-swizzled, K-major), so both MMAs take A and B
 // from shared memory.
 //
@@ -37,6 +40,7 @@
 // the host turns into NMFB_ETIMEOUT.  No TMA multicast is used.
 #include "nmfb_internal.cuh"
 #include "fused_common.cuh"
+#include "finish.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -96,7 +100,6 @@ struct GeoB {
     static_assert(VST >= 2, "shared-memory ring too small");
     static constexpr int SMEM = FIXED + 2 * XBYTES + YST * YSTAGE + NRB * RSTAGE + VST * VBYTES;
     static constexpr int NR = 16;                           // R warps
-    static constexpr int QW = BR / (NR / 4);                // 16 tile columns per R warp
     static constexpr int NTHR = (4 + NR + 4) * 32;
     static constexpr uint32_t ACCW = (MODE == 2 ? 2 : 1) * KP;   // TMEM columns of one accumulator
     static constexpr uint32_t DB0 = 2 * ACCW;               // Acc[0..1] at 0 and ACCW; D[b] at DB0 + b*BR
@@ -159,7 +162,6 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
 {
     using G = GeoB<KP, MODE>;
     constexpr int BR = G::BR;
-    constexpr int QW = G::QW;
     constexpr int NR = G::NR;
     constexpr bool SPLIT = MODE >= 1;                // MMA1 split
     constexpr bool SPLIT2 = MODE == 2;               // MMA2 split
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::VST; s++) {
             mbar_init(&vfull[s], 1);
-            mbar_init(&vempty[s], NR);
+            mbar_init(&vempty[s], NR / 2);   // one team reads each V tile
         }
         for (int s = 0; s < G::YST; s++) {
             mbar_init(&yfull[s], 1);
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
         }
         for (uint32_t b = 0; b < G::NDB; b++) mbar_init(&dfull[b], 1);
         for (int b = 0; b < G::NRB; b++) {
-            mbar_init(&rfull[b], NR);
+            mbar_init(&rfull[b], NR / 2);
             mbar_init(&rempty[b], 1);
         }
         for (int b = 0; b < 2; b++) {
@@ -367,11 +369,18 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
         }
     } else if (warp >= 4 && warp < 4 + NR) {
         // ------------------------------------------------------------ R warps
+        // Two teams of NR/2 warps take alternate tiles (team 0 even, team 1 odd), so
+        // one team's load latency overlaps the other's arithmetic; a warp handles
+        // TMEM lanes 32 quad .. +31 and CW tile columns in chunks of 16.
+        constexpr int GPT = NR / 8;                     // column groups per team
+        constexpr int CW = BR / GPT;                    // tile columns per warp
+        static_assert(CW % 16 == 0, "16-column chunks");
         uint32_t const quad = warp & 3;
-        uint32_t const half = (warp - 4) >> 2;          // column group (QW columns)
+        uint32_t const jg = (warp - 4) >> 2;
+        uint32_t const team = jg / GPT, grp = jg % GPT;
         uint32_t const row = quad * 32 + lane;          // TMEM lane = output row within the block
         uint32_t const lane_addr = tmem + ((quad * 32) << 16);
-        for (uint32_t t = 0; t < T; t++) {
+        for (uint32_t t = team; t < T; t += 2) {
             uint32_t const s = t % G::VST, b = t % G::NDB, rs = t % G::NRB;
             if (!mbar_wait(&dfull[b], (t / G::NDB) & 1, abort_flag, args.err, 25u, args.wait_ns)) break;
             if (!mbar_wait(&vfull[s], (t / G::VST) & 1, abort_flag, args.err, 26u, args.wait_ns)) break;
@@ -380,52 +389,58 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                 break;
             tc_fence_after();
             const unsigned char *sv = sV + s * G::VBYTES;
-            uint32_t d[32];
-            float v[QW];
-            tmem_ld16(lane_addr + G::DB0 + b * BR + half * QW, d);
-            if (HSIDE) {
-                // V tile [BR rows][128 cols], row-major; this thread's column = row.
-                const float *vs = reinterpret_cast<const float *>(sv) + (half * QW) * BO + row;
+#pragma unroll 1
+            for (int ch = 0; ch < CW / 16; ch++) {
+                int const col0 = grp * CW + ch * 16;
+                uint32_t d[32];
+                float v[16];
+                tmem_ld16(lane_addr + G::DB0 + b * BR + col0, d);
+                if (HSIDE) {
+                    // V tile [BR rows][128 cols], row-major; this thread's column = row.
+                    const float *vs = reinterpret_cast<const float *>(sv) + col0 * BO + row;
 #pragma unroll
-                for (int c = 0; c < QW; c++) v[c] = vs[c * BO];
-            } else {
-                // V boxes of [128 rows][32 floats], 128B swizzle; this warp's QW columns.
-                int const qb = (half * QW) / 32;
-                int const c0 = ((half * QW) % 32) / 4;
-                const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
+                    for (int c = 0; c < 16; c++) v[c] = vs[c * BO];
+                } else {
+                    // V boxes of [128 rows][32 floats], 128B swizzle.
+                    int const qb = col0 / 32;
+                    int const c0 = (col0 % 32) / 4;
+                    const unsigned char *vb = sv + qb * (BO * 128) + row * 128;
 #pragma unroll
-                for (int c = 0; c < QW / 4; c++) {
-                    float4 const x = *reinterpret_cast<const float4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
-                    v[4 * c + 0] = x.x;
-                    v[4 * c + 1] = x.y;
-                    v[4 * c + 2] = x.z;
-                    v[4 * c + 3] = x.w;
+                    for (int c = 0; c < 4; c++) {
+                        float4 const x = *reinterpret_cast<const float4 *>(vb + (((c + c0) ^ (row & 7)) << 4));
+                        v[4 * c + 0] = x.x;
+                        v[4 * c + 1] = x.y;
+                        v[4 * c + 2] = x.z;
+                        v[4 * c + 3] = x.w;
+                    }
                 }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&vempty[s]);
-            tmem_wait_ld_dep(d);
-            uint32_t pk[QW / 2], pl[QW / 2];
-#pragma unroll
-            for (int c = 0; c < QW; c += 2) {
-                // R = V * min(1/WH, FLT_MAX): zero-filled tile edges stay 0.
-                float const r0 = v[c] * fminf(rcp_approx(__uint_as_float(d[c])), FLT_MAX);
-                float const r1 = v[c + 1] * fminf(rcp_approx(__uint_as_float(d[c + 1])), FLT_MAX);
-                pk[c / 2] = pack_bf16x2(r0, r1);
-                if (SPLIT2) {
-                    float const h0 = __uint_as_float(pk[c / 2] << 16), h1 = __uint_as_float(pk[c / 2] & 0xffff0000u);
-                    pl[c / 2] = pack_bf16x2(r0 - h0, r1 - h1);
+                if (ch == CW / 16 - 1) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&vempty[s]);
                 }
-            }
-            // R row `row`, columns half*QW .. +QW: 16-byte chunks of a 128-byte K-major row, 128B swizzle.
-            unsigned char *rrow = sR + rs * G::RSTAGE + row * 128;
+                tmem_wait_ld_dep(d);
+                uint32_t pk[8], pl[8];
 #pragma unroll
-            for (int q = 0; q < QW / 8; q++) {
-                uint32_t const off = (((half * QW) / 8 + q) ^ (row & 7)) << 4;
-                *reinterpret_cast<uint4 *>(rrow + off) = make_uint4(pk[4 * q + 0], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
-                if (SPLIT2)
-                    *reinterpret_cast<uint4 *>(rrow + G::RBYTES + off) =
-                        make_uint4(pl[4 * q + 0], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
+                for (int c = 0; c < 16; c += 2) {
+                    // R = V * min(1/WH, FLT_MAX): zero-filled tile edges stay 0.
+                    float const r0 = v[c] * fminf(rcp_approx(__uint_as_float(d[c])), FLT_MAX);
+                    float const r1 = v[c + 1] * fminf(rcp_approx(__uint_as_float(d[c + 1])), FLT_MAX);
+                    pk[c / 2] = pack_bf16x2(r0, r1);
+                    if (SPLIT2) {
+                        float const h0 = __uint_as_float(pk[c / 2] << 16), h1 = __uint_as_float(pk[c / 2] & 0xffff0000u);
+                        pl[c / 2] = pack_bf16x2(r0 - h0, r1 - h1);
+                    }
+                }
+                // R row `row`, columns col0 .. +16: 16-byte chunks of a 128-byte K-major row, 128B swizzle.
+                unsigned char *rrow = sR + rs * G::RSTAGE + row * 128;
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    uint32_t const off = ((col0 / 8 + q) ^ (row & 7)) << 4;
+                    *reinterpret_cast<uint4 *>(rrow + off) = make_uint4(pk[4 * q + 0], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+                    if (SPLIT2)
+                        *reinterpret_cast<uint4 *>(rrow + G::RBYTES + off) =
+                            make_uint4(pl[4 * q + 0], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tc_fence_before();
@@ -523,6 +538,9 @@ struct PlanB {
     __nv_bfloat16 *wsplit, *hsplit;   // hi | lo | transposed hi/lo blocks, for W and for H
     uint32_t *dErr;                   // shared with the FP32 arm's error word
     int arm;                          // arm the Y^T maps were encoded for
+    double *dCs;                      // k_finish's column-sum partials (row blocks, then chunks)
+    uint32_t *dTick;                  // k_finish's retirement counters
+    uint32_t nticks, csoff;
 };
 
 template <int KP, int MODE>
@@ -651,26 +669,73 @@ int encode_maps_b(nmfb_ctx *ctx, PlanB *plan)
     return NMFB_OK;
 }
 
+// A factor's BF16 copies (hi, lo, transposed blocks) and column sums, when the
+// previous half-iteration's k_finish did not produce them.
+int prepare_b(nmfb_ctx *ctx, bool w)
+{
+    PlanB *plan = (PlanB *)ctx->bplan;
+    const float *F = w ? ctx->dW : ctx->dH;
+    uint32_t const rows = w ? ctx->n : ctx->m;
+    int rc = nmfb_colsum(ctx, F, rows, w ? ctx->dAccW : ctx->dAccH, w ? 0 : 1);
+    if (!rc) rc = split_factor(ctx, F, rows, w ? plan->wsplit : plan->hsplit, true);
+    if (!rc) ctx->fz_ok[w ? 0 : 1] = 1;
+    return rc;
+}
+
+template <int KP>
+int launch_finish_b(nmfb_ctx *ctx, bool is_H, uint32_t nsplit, int adjust)
+{
+    PlanB *plan = (PlanB *)ctx->bplan;
+    uint32_t const O = is_H ? ctx->m : ctx->n;
+    uint32_t const oblocks = (O + BO - 1) / BO;
+    if (oblocks > plan->csoff || (oblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
+        return nmfb_fail(ctx, NMFB_EINVAL, "bf16 arms: column-sum buffers too small");
+    __nv_bfloat16 *xs = is_H ? plan->hsplit : plan->wsplit;
+    size_t const sz = (size_t)O * KP;
+    FinishArgs fa = {};
+    fa.O = O;
+    fa.nsplit = nsplit;
+    fa.k = ctx->k;
+    fa.adjust = adjust;
+    fa.part = ctx->dPart;
+    fa.X = is_H ? ctx->dH : ctx->dW;
+    fa.accY = is_H ? ctx->dAccW : ctx->dAccH;
+    fa.bhi = xs;
+    fa.blo = xs + sz;
+    fa.bT = xs + 2 * sz;
+    fa.bnblk64 = (O + 63) / 64;
+    fa.cs = plan->dCs;
+    fa.csoff = plan->csoff;
+    fa.accX = is_H ? ctx->dAccH : ctx->dAccW;
+    fa.tick = plan->dTick;
+    fa.st = ctx->dState;
+    k_finish<KP, 64, 1><<<oblocks, 512, 0, ctx->stream>>>(fa);
+    NMFB_LAUNCH_CHECK(ctx);
+    return NMFB_OK;
+}
+
+// One half-iteration: the fused BF16 kernel and k_finish (which writes X's BF16
+// copies and column sums for the next half-iteration); the copies of X and Y
+// are prepared first only when they are not current.
 int bf16_half(nmfb_ctx *ctx, bool is_H, int adjust)
 {
     PlanB *plan = (PlanB *)ctx->bplan;
     if (!plan) return nmfb_fail(ctx, NMFB_ESTATE, "bf16 arm not prepared");
     int rc;
     if (plan->arm != ctx->arm && (rc = encode_maps_b(ctx, plan))) return rc;
-    float *X = is_H ? ctx->dH : ctx->dW;
-    const float *Y = is_H ? ctx->dW : ctx->dH;
-    uint32_t const xrows = is_H ? ctx->m : ctx->n;
-    uint32_t const yrows = is_H ? ctx->n : ctx->m;
-    float *acc = is_H ? ctx->dAccW : ctx->dAccH;
     int const whole = is_H ? 2 : 3;
     if ((rc = nmfb_prof_begin(ctx, whole))) return rc;
-    if ((rc = nmfb_colsum(ctx, Y, yrows, acc, is_H ? 0 : 1))) return rc;
-    if ((rc = split_factor(ctx, Y, yrows, is_H ? plan->wsplit : plan->hsplit, true))) return rc;
-    if ((rc = split_factor(ctx, X, xrows, is_H ? plan->hsplit : plan->wsplit, false))) return rc;
+    if (!ctx->fz_ok[is_H ? 0 : 1] && (rc = prepare_b(ctx, is_H))) return rc;    // Y
+    if (!ctx->fz_ok[is_H ? 1 : 0] && (rc = prepare_b(ctx, !is_H))) return rc;   // X
     int const nsplit = is_H ? dispatch_b<true>(ctx, plan->mapsH, plan->dErr) : dispatch_b<false>(ctx, plan->mapsW, plan->dErr);
     if (nsplit < 0) return nsplit;
-    rc = nmfb_muldiv(ctx, X, xrows, ctx->dPart, (uint32_t)nsplit, (size_t)xrows * ctx->kp, acc, adjust);
+    switch (ctx->kp) {
+    case 16: rc = launch_finish_b<16>(ctx, is_H, (uint32_t)nsplit, adjust); break;
+    case 32: rc = launch_finish_b<32>(ctx, is_H, (uint32_t)nsplit, adjust); break;
+    default: rc = launch_finish_b<64>(ctx, is_H, (uint32_t)nsplit, adjust); break;
+    }
     if (rc) return rc;
+    ctx->fz_ok[is_H ? 1 : 0] = 1;
     return nmfb_prof_end(ctx, whole);
 }
 
@@ -695,7 +760,14 @@ int nmfb_bf16_prepare(nmfb_ctx *ctx)
     size_t const wt = (size_t)((ctx->n + 63) / 64) * 128 * kp, ht = (size_t)((ctx->m + 63) / 64) * 128 * kp;
     cudaError_t e = nmfb_malloc(ctx, (void **)&plan->wsplit, (2 * wsz + wt) * sizeof(__nv_bfloat16));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->hsplit, (2 * hsz + ht) * sizeof(__nv_bfloat16));
+    uint32_t const maxblk = ((ctx->n > ctx->m ? ctx->n : ctx->m) + BO - 1) / BO;
+    plan->csoff = maxblk;
+    plan->nticks = (maxblk + FIN_ECH - 1) / FIN_ECH + 1;
+    if (e == cudaSuccess)
+        e = nmfb_malloc(ctx, (void **)&plan->dCs, (size_t)(maxblk + (maxblk + FIN_ECH - 1) / FIN_ECH) * kp * sizeof(double));
+    if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dTick, plan->nticks * sizeof(uint32_t));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "bf16 split buffers: %s", cudaGetErrorString(e));
+    NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dTick, 0, plan->nticks * sizeof(uint32_t), ctx->own_stream));
     return NMFB_OK;
 }
 
@@ -705,6 +777,8 @@ int nmfb_bf16_release(nmfb_ctx *ctx)
     if (!plan) return NMFB_OK;
     if (plan->wsplit) nmfb_free(ctx, plan->wsplit);
     if (plan->hsplit) nmfb_free(ctx, plan->hsplit);
+    if (plan->dCs) nmfb_free(ctx, plan->dCs);
+    if (plan->dTick) nmfb_free(ctx, plan->dTick);
     free(plan);
     ctx->bplan = nullptr;
     return NMFB_OK;
@@ -712,3 +786,11 @@ int nmfb_bf16_release(nmfb_ctx *ctx)
 
 int nmfb_bf16_update_H(nmfb_ctx *ctx, int adjust) { return bf16_half(ctx, true, adjust); }
 int nmfb_bf16_update_W(nmfb_ctx *ctx, int adjust) { return bf16_half(ctx, false, adjust); }
+
+// Makes W's BF16 copies and column sums current (before a test block is
+// replayed as a graph).
+int nmfb_bf16_ready_W(nmfb_ctx *ctx)
+{
+    if (!ctx->bplan || ctx->fz_ok[0]) return NMFB_OK;
+    return prepare_b(ctx, true);
+}

@@ -52,6 +52,7 @@
 // No TMA multicast is used anywhere.
 #include "nmfb_internal.cuh"
 #include "fused_common.cuh"
+#include "finish.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -96,8 +97,6 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t *r)
                  "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
                  : "memory");
 }
-
-constexpr uint32_t ECH = 32;   // row blocks per chunk of k_finish's column sums
 
 // Swizzle of a K-major operand whose rows are `bytes` long: the UMMA layout code
 // and the tensor-map mode (rows of 32 / 64 / 128 bytes).
@@ -217,189 +216,6 @@ __global__ void __launch_bounds__(256) k_split_factor(const float *__restrict__ 
     }
     __nv_bfloat16 *bt = BT + (size_t)blockIdx.x * kp * br;
     for (uint32_t e = threadIdx.x; e < kp * br; e += blockDim.x) bt[e] = tb[e % br][e / br];
-}
-
-// Finish of a half-iteration, one CTA of 512 threads per 128-row block of X
-// (four threads per row, a quarter of its columns each), right after k_fused_half:
-//   Xaux = the split partials summed in split order; X = X * Xaux / accY
-//   (matrix_mul_div, src/GPU_kernels.cu:1885-2058: product first, then the
-//   division, correctly rounded) with the EPS adjust when asked (kernel_adjust,
-//   :2338-2345); then X's split copies in k_split_factor's layout and its column
-//   sums (matrix_to_row, src/GPU_kernels.cu:871-1066) in FP64: a shuffle tree over
-//   each warp's 8 rows, the 16 warps in order, row blocks in chunks of ECH in block order,
-//   the chunks in order -- fixed orders throughout, so the result does not depend
-//   on scheduling.  It replaces the reference's mul_div + adjust and, for the next
-//   half-iteration, its column sums, in one launch.
-struct FinishArgs {
-    uint32_t O, nsplit, k;
-    int adjust;
-    const float *part;    // [split][O][KP]
-    float *X;
-    const float *accY;    // column sums of Y (KP)
-    float *xhi, *xT;      // X's split copies (SplitLayout of X's rows)
-    __nv_bfloat16 *xBl, *xB, *xBT;
-    uint32_t xnblk32, xnblkbr;
-    double *cs;           // [row block][KP] FP64 column-sum partials, then from row csoff [chunk][KP]
-    uint32_t csoff;
-    float *accX;          // column sums of the new X (KP)
-    uint32_t *tick;       // [chunks + 1] retirement counters (left at 0)
-    const ConvState *st;
-};
-
-template <int KP>
-__global__ void __launch_bounds__(512) k_finish(const FinishArgs a)
-{
-    constexpr int BR = Geo<KP>::BR;
-    constexpr int CPT = KP / 4;          // columns per thread (4 threads per row)
-    constexpr int NW = 16;               // warps
-    if (a.st && *(volatile const uint32_t *)&a.st->converged) return;
-    __shared__ double ws[NW * KP + 512];
-    __shared__ uint32_t eflag;
-    uint32_t const tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
-    uint32_t const row = tid / 4, c0 = (tid % 4) * CPT;
-    uint32_t const oblk = blockIdx.x, nob = gridDim.x;
-    uint32_t const o = oblk * BO + row;
-    bool const in = o < a.O;
-    float x[CPT];
-#pragma unroll
-    for (int c = 0; c < CPT; c++) x[c] = 0.0f;
-    if (in) {
-        // Xaux: the split partials in split order, loads issued four splits at a time
-        const float *pr = a.part + (size_t)o * KP + c0;
-        size_t const qs = (size_t)a.O * KP;
-        uint32_t q = 0;
-        for (; q + 4 <= a.nsplit; q += 4) {
-            float4 v[4][CPT / 4];
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-#pragma unroll
-                for (int c = 0; c < CPT / 4; c++) v[j][c] = __ldcg(reinterpret_cast<const float4 *>(pr + (q + j) * qs) + c);
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-#pragma unroll
-                for (int c = 0; c < CPT / 4; c++) {
-                    x[4 * c] += v[j][c].x;
-                    x[4 * c + 1] += v[j][c].y;
-                    x[4 * c + 2] += v[j][c].z;
-                    x[4 * c + 3] += v[j][c].w;
-                }
-        }
-        for (; q < a.nsplit; q++) {
-#pragma unroll
-            for (int c = 0; c < CPT / 4; c++) {
-                float4 const v = __ldcg(reinterpret_cast<const float4 *>(pr + q * qs) + c);
-                x[4 * c] += v.x;
-                x[4 * c + 1] += v.y;
-                x[4 * c + 2] += v.z;
-                x[4 * c + 3] += v.w;
-            }
-        }
-        float *xr = a.X + (size_t)o * KP + c0;
-#pragma unroll
-        for (int c = 0; c < CPT; c += 4) {
-            float4 const xv = *reinterpret_cast<const float4 *>(xr + c);
-            float const xs[4] = {xv.x, xv.y, xv.z, xv.w};
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                uint32_t const cc = c0 + c + i;
-                float v = 0.0f;
-                if (cc < a.k) {
-                    v = __fdiv_rn(xs[i] * x[c + i], __ldg(a.accY + cc));
-                    if (a.adjust) v = fmaxf(v, FLT_MIN);
-                }
-                x[c + i] = v;
-            }
-            *reinterpret_cast<float4 *>(xr + c) = make_float4(x[c], x[c + 1], x[c + 2], x[c + 3]);
-        }
-    }
-    // split copies; rows past the end are zero in the transposed blocks that exist
-    {
-        uint32_t const b32 = o / 32, bbr = o / BR;
-        bool const tin = b32 < a.xnblk32, btin = bbr < a.xnblkbr;
-        float *T32 = a.xT + (size_t)b32 * 2 * KP * 32 + (o % 32);
-        __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + (o % BR);
-#pragma unroll
-        for (int c = 0; c < CPT; c += 4) {
-            float h[4], l[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                h[i] = tf32_rna(x[c + i]);
-                l[i] = x[c + i] - h[i];
-            }
-            if (in) {
-                size_t const e = (size_t)o * KP + c0 + c;
-                *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(bf16x2_rn(l[0], l[1]), bf16x2_rn(l[2], l[3]));
-                *reinterpret_cast<uint2 *>(a.xB + e) = make_uint2(bf16x2_rn(x[c], x[c + 1]), bf16x2_rn(x[c + 2], x[c + 3]));
-            }
-            if (tin) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    T32[(c0 + c + i) * 32] = h[i];
-                    T32[(KP + c0 + c + i) * 32] = l[i];
-                }
-            }
-            if (btin) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) BT[(c0 + c + i) * BR] = __float2bfloat16_rn(x[c + i]);
-            }
-        }
-    }
-    // column sums of this row block: the warp's 8 rows of each column by a shuffle
-    // tree (lanes 4r + g hold row r, column group g), then the 16 warps in order
-#pragma unroll
-    for (int c = 0; c < CPT; c++) {
-        double v = (double)x[c];
-#pragma unroll
-        for (int off = 16; off >= 4; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane < 4) ws[warp * KP + c0 + c] = v;
-    }
-    __syncthreads();
-    if (tid < (uint32_t)KP) {
-        double t = 0.0;
-#pragma unroll
-        for (int w = 0; w < NW; w++) t += ws[w * KP + tid];
-        a.cs[(size_t)oblk * KP + tid] = t;
-    }
-    __threadfence();
-    __syncthreads();
-    uint32_t const nch = (nob + ECH - 1) / ECH, ch = oblk / ECH;
-    uint32_t const b0 = ch * ECH, bn = min(nob - b0, ECH);
-    if (tid == 0) eflag = (atomicAdd(&a.tick[ch], 1u) == bn - 1) ? 1u : 0u;
-    __syncthreads();
-    if (!eflag) return;
-    // last row block of its chunk: the chunk's partials in block order
-    __threadfence();
-    constexpr int GRP = 512 / KP;
-    uint32_t const g = tid / KP, c = tid % KP;
-    double t = 0.0;
-    for (uint32_t blk = g; blk < bn; blk += GRP) t += __ldcg(a.cs + (size_t)(b0 + blk) * KP + c);
-    ws[NW * KP + tid] = t;
-    __syncthreads();
-    if (tid < (uint32_t)KP) {
-        double u = 0.0;
-        for (int gg = 0; gg < GRP; gg++) u += ws[NW * KP + gg * KP + tid];
-        a.cs[((size_t)a.csoff + ch) * KP + tid] = u;
-    }
-    if (tid == 0) a.tick[ch] = 0u;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) eflag = (atomicAdd(&a.tick[nch], 1u) == nch - 1) ? 1u : 0u;
-    __syncthreads();
-    if (!eflag) return;
-    // last chunk: the chunk sums in order
-    __threadfence();
-    double v = 0.0;
-    for (uint32_t q = g; q < nch; q += GRP) v += __ldcg(a.cs + ((size_t)a.csoff + q) * KP + c);
-    __syncthreads();
-    ws[NW * KP + tid] = v;
-    __syncthreads();
-    if (tid < (uint32_t)KP) {
-        double u = 0.0;
-        for (int gg = 0; gg < GRP; gg++) u += ws[NW * KP + gg * KP + tid];
-        a.accX[tid] = (float)u;
-    }
-    if (tid == 0) a.tick[nch] = 0u;
 }
 
 // Warp roles: 0 = V producer (TMA), 1 = MMA issuer + TMEM owner, 2 = X and Y
@@ -993,9 +809,9 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
     fa.accX = HSIDE ? ctx->dAccH : ctx->dAccW;
     fa.tick = plan->dTick;
     fa.st = ctx->dState;
-    if (oblocks > plan->csoff || (oblocks + ECH - 1) / ECH + 1 > plan->nticks)
+    if (oblocks > plan->csoff || (oblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
         return nmfb_fail(ctx, NMFB_EINVAL, "fused: column-sum buffers too small");
-    k_finish<KP><<<oblocks, 512, 0, ctx->stream>>>(fa);
+    k_finish<KP, BR, 0><<<oblocks, 512, 0, ctx->stream>>>(fa);
     NMFB_LAUNCH_CHECK(ctx);
     return (int)nsplit;
 }
@@ -1093,9 +909,9 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, LH.floats * sizeof(float));
     uint32_t const maxblk = ((ctx->n > ctx->m ? ctx->n : ctx->m) + BO - 1) / BO;
     plan->csoff = maxblk;
-    plan->nticks = (maxblk + ECH - 1) / ECH + 1;
+    plan->nticks = (maxblk + FIN_ECH - 1) / FIN_ECH + 1;
     if (e == cudaSuccess)
-        e = nmfb_malloc(ctx, (void **)&plan->dCs, (size_t)(maxblk + (maxblk + ECH - 1) / ECH) * kp * sizeof(double));
+        e = nmfb_malloc(ctx, (void **)&plan->dCs, (size_t)(maxblk + (maxblk + FIN_ECH - 1) / FIN_ECH) * kp * sizeof(double));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dTick, plan->nticks * sizeof(uint32_t));
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ENOMEM, "fused split buffers: %s", cudaGetErrorString(e));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(plan->dTick, 0, plan->nticks * sizeof(uint32_t), ctx->own_stream));

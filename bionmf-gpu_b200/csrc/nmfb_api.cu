@@ -492,7 +492,9 @@ static int launch_block(nmfb_ctx *ctx, uint32_t J)
     static int const use_graphs = getenv("NMFB_NO_GRAPHS") == nullptr;
     if (!use_graphs || ctx->prof_on || ctx->splan) return enqueue_block(ctx, J);
     // the graph holds no preparation launch: make W's split copies current first
-    int const rc0 = (ctx->arm == NMFB_ARM_FUSED || ctx->arm == NMFB_ARM_FUSED_TF32) ? nmfb_fused_ready_W(ctx) : NMFB_OK;
+    int const rc0 = (ctx->arm == NMFB_ARM_FUSED || ctx->arm == NMFB_ARM_FUSED_TF32) ? nmfb_fused_ready_W(ctx)
+                    : ctx->arm >= NMFB_ARM_BF16                                    ? nmfb_bf16_ready_W(ctx)
+                                                                                   : NMFB_OK;
     if (rc0) return rc0;
     if (!ctx->blk_exec || ctx->blk_J != J || ctx->blk_arm != ctx->arm || ctx->blk_stream != ctx->stream ||
         ctx->blk_wait != ctx->wait_ns) {

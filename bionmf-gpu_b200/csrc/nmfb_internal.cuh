@@ -56,7 +56,7 @@ struct nmfb_ctx {
     nmfb::ConvState *dState;
     nmfb::ConvState *hState;  // pinned host mirror
 
-    // Fused arm: the split copies and column sums of W ([0]) and of H ([1]) match
+    // Fused arms: the split copies and column sums of W ([0]) and of H ([1]) match
     // the factor (written by the previous half-iteration's epilogue).  Trusted
     // only inside one nmfb_run or step call; every entry point starts from 0.
     int fz_ok[2];
@@ -161,6 +161,7 @@ int nmfb_bf16_prepare(nmfb_ctx *ctx);
 int nmfb_bf16_release(nmfb_ctx *ctx);
 int nmfb_bf16_update_H(nmfb_ctx *ctx, int adjust);
 int nmfb_bf16_update_W(nmfb_ctx *ctx, int adjust);
+int nmfb_bf16_ready_W(nmfb_ctx *ctx);
 
 // Max number of reduction splits used by any arm (sizes dPart).
 #define NMFB_MAX_SPLIT 64

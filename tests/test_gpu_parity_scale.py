@@ -20,7 +20,7 @@ trajectories differ by up to 2e-4 in KL); classification bit-exact on every
 sample whose top two factor loadings differ by more than 1e-3 (closer ones
 are ties at the factors' own tolerance; at least 99 % of samples qualify,
 90 % after the headline case's three iterations from the random start).  The
-BF16x3 arm is held to its stated bounds (W / H 1e-3, KL 1e-5).
+reduced-precision arms are held to the bounds listed at ARM_BOUNDS.
 """
 from __future__ import annotations
 
@@ -88,18 +88,30 @@ def _c_submatrix_oracle(oracle, synth, k):
     return _SUB[k]
 
 
-@pytest.mark.parametrize("arm,wtol", [("fused", 1e-4), ("bf16x3", 1e-3)])
+# Every arm against FP64 on the C-submatrix: W / H after 20 iterations and the
+# final divergence.  The FP32-class arms (fused, BF16x3) are held to the
+# method's bounds (W / H 1e-4, KL 1e-5) and bit-exact classification; the
+# reduced-precision arms to bounds a few times their measured errors (measured
+# on a B200 at k = 32 / 64: split-BF16 W 2.2e-3 / 7.7e-4, KL 8.6e-5 / 9.0e-5;
+# BF16 W 2.4e-3 / 9.1e-4, KL 5.3e-4 / 7.4e-4; 1xTF32 W 2.6e-4 / 1.5e-4,
+# KL 6.1e-6 / 8.6e-6).
+ARM_BOUNDS = [("fused", 1e-4, 1e-5), ("bf16x3", 1e-4, 1e-5), ("split_bf16", 1e-2, 5e-4),
+              ("bf16", 1e-2, 3e-3), ("fused_tf32", 2e-3, 1e-4)]
+
+
+@pytest.mark.parametrize("arm,wtol,kltol", ARM_BOUNDS)
 @pytest.mark.parametrize("k", [32, 64])
-def test_c_submatrix(pkg, oracle, synth, arm, wtol, k):
+def test_c_submatrix(pkg, oracle, synth, arm, wtol, kltol, k):
     V, W64, H64, kl64 = _c_submatrix_oracle(oracle, synth, k)
     # fixed count: factors
     W, H, lab, _ = _run(pkg, V, k, arm, 20)
     assert maxnorm_rel(W, W64) < wtol
     assert maxnorm_rel(H, H64) < wtol
-    assert_labels_match(lab, H64, oracle.classify)
+    if wtol <= 1e-4:
+        assert_labels_match(lab, H64, oracle.classify)
     # final divergence, once it has settled
     _, _, _, kl = _run(pkg, V, k, arm, KL_ITERS)
-    assert abs(kl - kl64) <= 1e-5 * abs(kl64)
+    assert abs(kl - kl64) <= kltol * abs(kl64)
 
 
 def test_config_b_fixed_iterations(pkg, oracle, synth):
