@@ -519,7 +519,7 @@ def stream_rates(dev, iters=10):
                     "link-bound and linear in bytes, so its per-iteration time is extrapolated"}
 
 
-SERVE = {"requests": 300, "pool": 32, "n": (1000, 50000), "m": (20, 2000), "k": (2, 20), "iters": 300,
+SERVE = {"requests": 2000, "pool": 32, "n": (1000, 50000), "m": (20, 2000), "k": (2, 20), "iters": 300,
          "budget_gb": 120.0, "workers": 32, "load": 0.8,
          "desc": "requests n~U[1000,50000], m~logU[20,2000], k~U[2,20], planted Poisson V, 300-iteration cap "
                  "(-j 10 -t 40: no request can converge before 410 iterations), 120 GB budget"}
@@ -552,10 +552,12 @@ def serve_requests(dev, count, seed=11):
 
 
 def serve_rates(dev, count=None, seq_sample=40):
-    """Serving loop: capacity (all requests queued at once), the sequential
-    baseline (one request at a time, same engine), and an open-loop run with
-    Poisson arrivals at SERVE['load'] of the measured capacity (p50 / p99
-    latency from arrival to result on the host)."""
+    """Serving loop on config E's 2000 requests: capacity (all requests queued
+    at once), the sequential baseline (one request at a time, same engine, a
+    sample), and an open-loop run of all requests with Poisson arrivals at
+    SERVE['load'] of the measured capacity (p50 / p99 latency from arrival to
+    result on the host); the device queue and a half-load point on the first
+    requests only, to keep the line within minutes."""
     _import_package()
     import nmf_b200.serve as serve
     count = count or SERVE["requests"]
@@ -567,18 +569,18 @@ def serve_rates(dev, count=None, seq_sample=40):
     # requests it takes (m <= 256)
     qsrv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
                         batched=True)
-    small = [r for r in reqs if qsrv._queued(r)]
+    small = [r for r in reqs[:300] if qsrv._queued(r)]
     qsrv.run(small[:8], open_loop=False)
     q_small = qsrv.run(small, open_loop=False)
     c_small = srv.run(small, open_loop=False)
     seq = srv.run_sequential(reqs[:seq_sample])
     open_runs = {}
-    for load in (SERVE["load"], 0.5):
+    for load, part in ((SERVE["load"], reqs), (0.5, reqs[:300])):
         rate = load * cap.solves_per_s()
-        arr = serve.poisson_arrivals(count, rate, seed=5)
-        for r, t in zip(reqs, arr):
+        arr = serve.poisson_arrivals(len(part), rate, seed=5)
+        for r, t in zip(part, arr):
             r.arrival = float(t)
-        st = srv.run(reqs, open_loop=True)
+        st = srv.run(part, open_loop=True)
         open_runs[load] = (rate, st)
     rate, op = open_runs[SERVE["load"]]
     rate50, op50 = open_runs[0.5]
@@ -591,10 +593,10 @@ def serve_rates(dev, count=None, seq_sample=40):
                              "p50_s": q_small.latency_pct(50), "p99_s": q_small.latency_pct(99),
                              "note": "the requests with m <= 256, all queued at t = 0: persistent serving kernel "
                                      "vs per-request contexts"},
-            "open_loop": {"arrival_rate": rate, "solves_s": op.solves_per_s(), "p50_s": op.latency_pct(50),
+            "open_loop": {"requests": count, "arrival_rate": rate, "solves_s": op.solves_per_s(), "p50_s": op.latency_pct(50),
                           "p99_s": op.latency_pct(99), "peak_active": op.peak_active,
                           "peak_gb": op.peak_bytes / 1e9},
-            "open_loop_half_load": {"arrival_rate": rate50, "solves_s": op50.solves_per_s(),
+            "open_loop_half_load": {"requests": 300, "arrival_rate": rate50, "solves_s": op50.solves_per_s(),
                                     "p50_s": op50.latency_pct(50), "p99_s": op50.latency_pct(99)},
             "sequential_p50_s_per_request": float(np.median([r.done - r.admitted for r in seq.results])),
             "workers": SERVE["workers"]}

@@ -547,6 +547,10 @@ __device__ void run_problem(Problem &P, float *sm, uint32_t *s_ctl, const Slice 
     __syncthreads();
 }
 
+// KMAX: the largest rank the instantiation handles (10 or 20).  A batch whose
+// ranks are all <= 10 (a rank sweep) runs the 10-rank variant: without the
+// k = 11..20 paths in the kernel, its registers are allocated for k <= 10.
+template <int KMAX>
 __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, const uint32_t *__restrict__ order,
                                                  uint32_t nprob, uint32_t *__restrict__ queue)
 {
@@ -578,11 +582,21 @@ __global__ void __launch_bounds__(NT, 2) k_batch(Problem *__restrict__ probs, co
 #define NMFB_BATCH_CASE(KK) \
     case KK: run_problem<KK>(P, sm, s_ctl, X); break;
             NMFB_BATCH_CASE(2) NMFB_BATCH_CASE(3) NMFB_BATCH_CASE(4) NMFB_BATCH_CASE(5) NMFB_BATCH_CASE(6)
-            NMFB_BATCH_CASE(7) NMFB_BATCH_CASE(8) NMFB_BATCH_CASE(9) NMFB_BATCH_CASE(10) NMFB_BATCH_CASE(11)
-            NMFB_BATCH_CASE(12) NMFB_BATCH_CASE(13) NMFB_BATCH_CASE(14) NMFB_BATCH_CASE(15) NMFB_BATCH_CASE(16)
-            NMFB_BATCH_CASE(17) NMFB_BATCH_CASE(18) NMFB_BATCH_CASE(19) NMFB_BATCH_CASE(20)
+            NMFB_BATCH_CASE(7) NMFB_BATCH_CASE(8) NMFB_BATCH_CASE(9) NMFB_BATCH_CASE(10)
 #undef NMFB_BATCH_CASE
-            default: break;
+            default:
+                if (KMAX > 10) {
+                    switch (P.k) {
+#define NMFB_BATCH_CASE(KK) \
+    case KK: run_problem<(KMAX > 10 ? KK : 2)>(P, sm, s_ctl, X); break;
+                        NMFB_BATCH_CASE(11) NMFB_BATCH_CASE(12) NMFB_BATCH_CASE(13) NMFB_BATCH_CASE(14)
+                        NMFB_BATCH_CASE(15) NMFB_BATCH_CASE(16) NMFB_BATCH_CASE(17) NMFB_BATCH_CASE(18)
+                        NMFB_BATCH_CASE(19) NMFB_BATCH_CASE(20)
+#undef NMFB_BATCH_CASE
+                        default: break;
+                    }
+                }
+                break;
         }
         if (crank == 0 && threadIdx.x == 0) {
             Problem *dst = probs + order[q];
@@ -1135,9 +1149,12 @@ int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, ui
     BTRY(b, cudaMemcpyAsync(b->dProbs, P.data(), b->nprob * sizeof(Problem), cudaMemcpyHostToDevice, b->stream));
     BTRY(b, cudaMemcpyAsync(b->dOrder, order.data(), b->nprob * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     BTRY(b, cudaMemsetAsync(b->dQueue, 0, sizeof(uint32_t), b->stream));
-    BTRY(b, cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint32_t kmax = 0;
+    for (uint32_t p = 0; p < b->nprob; p++) kmax = std::max(kmax, b->ranks[p]);
+    auto const kern = kmax <= 10 ? k_batch<10> : k_batch<20>;
+    BTRY(b, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    BTRY(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, NT, smem));
+    BTRY(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     if (per_sm < 1) return bfail(b, NMFB_EINVAL, "batched kernel does not fit on an SM with %zu B shared memory", smem);
     // CTAs per problem: automatic = 8 when the batch leaves most CTA slots idle
     // at one problem per 8 CTAs, else 4 (a problem's time shrinks about C-fold,
@@ -1158,13 +1175,13 @@ int nmfb_batch_run(nmfb_batch *b, uint32_t n_iters, uint32_t niter_test_conv, ui
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    BTRY(b, cudaOccupancyMaxActiveClusters(&nclusters, k_batch, &cfg));
+    BTRY(b, cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg));
     if (nclusters < 1) return bfail(b, NMFB_EINVAL, "no cluster of %u batched CTAs fits on the device", C);
     uint32_t ncl = (uint32_t)nclusters < b->nprob ? (uint32_t)nclusters : b->nprob;
     cfg.gridDim = dim3(ncl * C, 1, 1);
     b->last_cluster = C;
     BTRY(b, cudaEventRecord(b->ev0, b->stream));
-    BTRY(b, cudaLaunchKernelEx(&cfg, k_batch, b->dProbs, (const uint32_t *)b->dOrder, b->nprob, b->dQueue));
+    BTRY(b, cudaLaunchKernelEx(&cfg, kern, b->dProbs, (const uint32_t *)b->dOrder, b->nprob, b->dQueue));
     BTRY(b, cudaEventRecord(b->ev1, b->stream));
     BTRY(b, cudaMemcpyAsync(P.data(), b->dProbs, b->nprob * sizeof(Problem), cudaMemcpyDeviceToHost, b->stream));
     BTRY(b, cudaStreamSynchronize(b->stream));
