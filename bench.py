@@ -521,6 +521,9 @@ def stream_rates(dev, iters=10):
 
 SERVE = {"requests": 2000, "pool": 32, "n": (1000, 50000), "m": (20, 2000), "k": (2, 20), "iters": 300,
          "budget_gb": 120.0, "workers": 32, "load": 0.8,
+         # SMs each request's context sizes its launches for: the best of 0 (all), 74, 37, 24
+         # and 16 on 400 requests of this mix (121 solves/s at 74 against 112 at 0)
+         "sm_limit": 74,
          "desc": "requests n~U[1000,50000], m~logU[20,2000], k~U[2,20], planted Poisson V, 300-iteration cap "
                  "(-j 10 -t 40: no request can converge before 410 iterations), 120 GB budget"}
 
@@ -562,7 +565,8 @@ def serve_rates(dev, count=None, seq_sample=40):
     import nmf_b200.serve as serve
     count = count or SERVE["requests"]
     reqs = serve_requests(dev, count)
-    srv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0)
+    srv = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
+                       sm_limit=SERVE["sm_limit"])
     srv.run(reqs[:8], open_loop=False)                       # warm-up (module loads, allocator pools)
     cap = srv.run(reqs, open_loop=False)
     # the device queue (persistent serving kernel) against contexts on the
@@ -599,7 +603,8 @@ def serve_rates(dev, count=None, seq_sample=40):
             "open_loop_half_load": {"requests": 300, "arrival_rate": rate50, "solves_s": op50.solves_per_s(),
                                     "p50_s": op50.latency_pct(50), "p99_s": op50.latency_pct(99)},
             "sequential_p50_s_per_request": float(np.median([r.done - r.admitted for r in seq.results])),
-            "workers": SERVE["workers"]}
+            "workers": SERVE["workers"], "sm_limit": SERVE["sm_limit"],
+            "sequential_note": "one request at a time, each context sized for all SMs"}
 
 
 SERVE_SMALL = {"requests": 400, "n": (500, 5000), "m": (20, 256), "k": (2, 10), "iters": 300,
@@ -625,7 +630,8 @@ def serve_small_rates(dev, seq_sample=40):
                                   stop_threshold=40, rid=i))
     q = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
                      batched=True)
-    c = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0)
+    c = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
+                     sm_limit=SERVE["sm_limit"])
     q.run(reqs[:8], open_loop=False)
     c.run(reqs[:8], open_loop=False)
     qs = q.run(reqs, open_loop=False)

@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH):
         "nmfb_synchronize": ([vp], i32),
         "nmfb_launch_count": ([vp], C.c_uint64),
         "nmfb_set_wait_limit": ([vp, C.c_uint64], i32),
+        "nmfb_set_sm_limit": ([vp, u32], i32),
         "nmfb_update_H_noalloc": ([vp, sz, vp, sz, vp, sz, u32, u32, u32, vp], i32),
         "nmfb_batch_create": ([C.POINTER(vp), i32, u32, u32, u32, C.POINTER(u32)], i32),
         "nmfb_batch_destroy": ([vp], i32),
@@ -322,6 +323,11 @@ class NMF:
     def set_wait_limit(self, ns: int):
         """Limit of the fused kernels' bounded device waits in ns (0: default, 1 s)."""
         self._check(self._L.nmfb_set_wait_limit(self._h, int(ns)))
+
+    def set_sm_limit(self, sms: int):
+        """Size this context's launches for `sms` SMs (0: the whole device), so
+        that several contexts' kernels can share the GPU side by side."""
+        self._check(self._L.nmfb_set_sm_limit(self._h, int(sms)))
 
 
 def _uptr(a: np.ndarray):

@@ -127,12 +127,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // 1/x with rcp.approx.ftz.f32 (PTX: at most 1 ulp of error); the quotient is
-// v * min(1/wh, FLT_MAX), so a zero denominator gives a finite result.
+// v * (1/wh).  Every element the loops visit is a real one (no zero padding),
+// so a zero denominator behaves as in the reference's division (v / 0 = inf,
+// 0 / 0 = NaN).
 __device__ __forceinline__ float quotient(float v, float wh)
 {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(wh));
-    return v * fminf(r, FLT_MAX);
+    return v * r;
 }
 
 // Load the first K of a 16-byte aligned row of KS floats with float4 loads.

@@ -389,6 +389,8 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                 break;
             tc_fence_after();
             const unsigned char *sv = sV + s * G::VBYTES;
+            bool const edge = (t_begin + t + 1) * BR > args.R;   // the partial last reduction tile
+            int const valid = (int)(args.R - (t_begin + t) * BR);          // its columns before R
 #pragma unroll 1
             for (int ch = 0; ch < CW / 16; ch++) {
                 int const col0 = grp * CW + ch * 16;
@@ -419,12 +421,22 @@ __global__ void __launch_bounds__(GeoB<KP, MODE>::NTHR, 1)
                     if (lane == 0) mbar_arrive(&vempty[s]);
                 }
                 tmem_wait_ld_dep(d);
+                if (edge) {
+                    // Columns past R are zero-filled (V = 0, WH = 0): WH = 1 there makes R 0
+                    // instead of 0 * inf, which the second contraction would carry into every row.
+#pragma unroll
+                    for (int c = 0; c < 16; c++)
+                        if (col0 + c >= valid) {
+                            d[c] = 0x3f800000u;
+                            v[c] = 0.0f;
+                        }
+                }
                 uint32_t pk[8], pl[8];
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
-                    // R = V * min(1/WH, FLT_MAX): zero-filled tile edges stay 0.
-                    float const r0 = v[c] * fminf(rcp_approx(__uint_as_float(d[c])), FLT_MAX);
-                    float const r1 = v[c + 1] * fminf(rcp_approx(__uint_as_float(d[c + 1])), FLT_MAX);
+                    // R = V * (1/WH); a zero WH of the data behaves as in the reference's division.
+                    float const r0 = v[c] * rcp_approx(__uint_as_float(d[c]));
+                    float const r1 = v[c + 1] * rcp_approx(__uint_as_float(d[c + 1]));
                     pk[c / 2] = pack_bf16x2(r0, r1);
                     if (SPLIT2) {
                         float const h0 = __uint_as_float(pk[c / 2] << 16), h1 = __uint_as_float(pk[c / 2] & 0xffff0000u);

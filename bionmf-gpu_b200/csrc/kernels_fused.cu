@@ -497,6 +497,8 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
             DBG_PH(2, t);
             if (warp == 4 && lane == 0) DBG_TS(5, t);
             const unsigned char *sv = sV + s * G::VBYTES;
+            bool const edge = (t_begin + t + 1) * BR > args.R;   // the partial last reduction tile
+            int const valid = (int)(args.R - (t_begin + t) * BR);          // its columns before R
 #pragma unroll 1
             for (int ch = 0; ch < CW / 16; ch++) {
                 int const col0 = grp * CW + ch * 16;                          // first tile column of the chunk
@@ -540,15 +542,25 @@ __global__ void __launch_bounds__(Geo<KP>::NTHR, 1)
                 }
                 tmem_wait_ld_dep(d);
                 if (ch == CW / 16 - 1) DBG_PH(4, t);
+                if (edge) {
+                    // Columns past R are zero-filled (V = 0, WH = 0): WH = 1 there makes R 0
+                    // instead of 0 * inf, which MMA2 would carry into every row's sum.
+#pragma unroll
+                    for (int c = 0; c < 16; c++)
+                        if (col0 + c >= valid) {
+                            d[c] = 0x3f800000u;
+                            v[c] = 0u;
+                        }
+                }
                 uint32_t pl[8];   // bf16(R lo), packed in column pairs
 #pragma unroll
                 for (int c = 0; c < 16; c++) {
                     // R = V / WH as V * (1/WH): the approximate reciprocal (<= 1 ulp) runs at
-                    // full rate, the fast-division intrinsic at a third of it.  min(., FLT_MAX)
-                    // keeps the zero-filled edges (V = 0, WH = 0) at 0 instead of 0 * inf.
+                    // full rate, the fast-division intrinsic at a third of it.  A zero WH of
+                    // the data behaves as in the reference's division (V / 0 = inf, 0 / 0 = NaN).
                     float const vv = __uint_as_float(v[c]);
                     float const wh = __uint_as_float(d[c]);
-                    float const r = vv * fminf(rcp_approx(wh), FLT_MAX);
+                    float const r = vv * rcp_approx(wh);
                     float const h = tf32_rna(r);
 #ifdef NMFB_FUSED_DEBUG
                     if (args.dbg && blockIdx.x == 0 && t == 0) {
@@ -750,15 +762,16 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
     uint32_t const T = (R + BR - 1) / BR;
     // Splits of the reduction: one CTA per SM at a time, so the launch takes
     // ceil(CTAs / SMs) waves of (tiles per split + pipeline fill) tile times;
-    // pick the split count that minimises that (fill ~ 3 tiles: TMEM
-    // allocation, X load and split, first MMA1, partial write).
+    // pick the split count that minimises that (fill ~ 6 tiles: TMEM
+    // allocation, X load and split, pipeline ramp, partial write; measured
+    // best among 1, 3 and 6).
     uint32_t tps = T, best = 0xffffffffu;
     for (uint32_t want = 1; want <= NMFB_MAX_SPLIT && want <= T; want++) {
         uint32_t const t_ps = (T + want - 1) / want;
         uint32_t const ns = (T + t_ps - 1) / t_ps;
         if ((size_t)ns * O * KP > ctx->part_items) break;
         uint32_t const waves = (oblocks * ns + (uint32_t)ctx->sm_count - 1) / (uint32_t)ctx->sm_count;
-        uint32_t const cost = waves * (t_ps + 3);
+        uint32_t const cost = waves * (t_ps + 6);
         if (cost < best) {
             best = cost;
             tps = t_ps;

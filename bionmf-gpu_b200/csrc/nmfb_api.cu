@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <mutex>
 #include <new>
+#include <vector>
 
 using nmfb::ConvState;
 
@@ -49,8 +50,71 @@ cudaError_t nmfb_malloc(nmfb_ctx *ctx, void **p, size_t bytes)
     return cudaMallocFromPoolAsync(p, bytes, pool, ctx->own_stream);
 }
 
+// Page-locked host staging buffers, shared by every context of the process.
+// Allocating or freeing page-locked memory is ordered against the work of all
+// streams of the device, so a context that did either for each upload or
+// download would stall the kernels of every other context in flight (many
+// solves served side by side); buffers taken from here are allocated once,
+// in power-of-two sizes, and reused.
+namespace {
+struct StageBuf {
+    void *p;
+    size_t bytes;
+    bool busy;
+};
+std::mutex g_stage_mutex;
+std::vector<StageBuf> g_stage;
+
+void *stage_get(size_t bytes)
+{
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    StageBuf *best = nullptr;
+    for (StageBuf &b : g_stage)
+        if (!b.busy && b.bytes >= bytes && (!best || b.bytes < best->bytes)) best = &b;
+    if (best) {
+        best->busy = true;
+        return best->p;
+    }
+    size_t sz = 4096;
+    while (sz < bytes) sz <<= 1;
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocPortable) != cudaSuccess) {   // usable by every device's context
+        cudaGetLastError();
+        return nullptr;
+    }
+    g_stage.push_back({p, sz, true});
+    return p;
+}
+
+void stage_put(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    for (StageBuf &b : g_stage)
+        if (b.p == p) {
+            b.busy = false;
+            return;
+        }
+}
+
+// Free the staging buffers no context holds.
+void stage_trim()
+{
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    std::vector<StageBuf> keep;
+    for (StageBuf &b : g_stage) {
+        if (b.busy)
+            keep.push_back(b);
+        else
+            cudaFreeHost(b.p);
+    }
+    g_stage.swap(keep);
+}
+}  // namespace
+
 int nmfb_release_cached(int device)
 {
+    stage_trim();
     cudaMemPool_t pool = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_pool_mutex);
@@ -112,7 +176,7 @@ void free_all(nmfb_ctx *ctx)
                     ctx->dFirst,   ctx->dLastRep, ctx->dState};
     for (void *b : bufs)
         if (b) nmfb_free(ctx, b);
-    if (ctx->hState) cudaFreeHost(ctx->hState);
+    stage_put(ctx->hState);
     nmfb_stream_release(ctx);
     nmfb_bf16_release(ctx);
     nmfb_fused_release(ctx);
@@ -130,8 +194,8 @@ void free_all(nmfb_ctx *ctx)
 int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, uint32_t cols, size_t ld)
 {
     size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
-    float *stage = nullptr;
-    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&stage, bytes));
+    float *stage = (float *)stage_get(bytes);
+    if (!stage) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked staging buffer of %zu bytes", bytes);
     for (uint32_t r = 0; r < rows; r++) {
         float *d = stage + (size_t)r * ctx->kp;
         memcpy(d, src + (size_t)r * ld, cols * sizeof(float));
@@ -139,7 +203,7 @@ int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, ui
     }
     cudaError_t e = cudaMemcpyAsync(dst, stage, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFreeHost(stage);
+    stage_put(stage);
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "upload: %s", cudaGetErrorString(e));
     return NMFB_OK;
 }
@@ -147,14 +211,56 @@ int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, ui
 int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, size_t ld)
 {
     size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
-    float *stage = nullptr;
-    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&stage, bytes));
+    float *stage = (float *)stage_get(bytes);
+    if (!stage) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked staging buffer of %zu bytes", bytes);
     cudaError_t e = cudaMemcpyAsync(stage, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess)
         for (uint32_t r = 0; r < rows; r++) memcpy(dst + (size_t)r * ld, stage + (size_t)r * ctx->kp, ctx->k * sizeof(float));
-    cudaFreeHost(stage);
+    stage_put(stage);
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "download: %s", cudaGetErrorString(e));
+    return NMFB_OK;
+}
+
+// Upload the host matrix V (n x m, ld) into the device's n x ldv layout: rows
+// are packed at the device pitch (padding zero) into two page-locked staging
+// buffers of at most 8 MB in turn, each copied with one DMA while the next is
+// filled.  (A pitched copy straight from pageable memory moves one short row
+// at a time.)
+int upload_V(nmfb_ctx *ctx, const float *V, size_t ld)
+{
+    size_t const row_bytes = ctx->ldv * sizeof(float);
+    uint32_t const per = (uint32_t)((size_t)(8u << 20) / row_bytes > 0 ? (size_t)(8u << 20) / row_bytes : 1);
+    uint32_t const rows = per < ctx->n ? per : ctx->n;
+    float *stage[2] = {(float *)stage_get(rows * row_bytes), (float *)stage_get(rows * row_bytes)};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaError_t e = (stage[0] && stage[1]) ? cudaSuccess : cudaErrorMemoryAllocation;
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+    uint32_t c = 0;
+    for (uint32_t r0 = 0; r0 < ctx->n && e == cudaSuccess; r0 += rows, c++) {
+        uint32_t const nr = ctx->n - r0 < rows ? ctx->n - r0 : rows;
+        float *const st = stage[c & 1];
+        if (c >= 2) e = cudaEventSynchronize(ev[c & 1]);   // the DMA of chunk c - 2 has read this buffer
+        if (e != cudaSuccess) break;
+        for (uint32_t r = 0; r < nr; r++) {
+            float *d = st + (size_t)r * ctx->ldv;
+            memcpy(d, V + (size_t)(r0 + r) * ld, ctx->m * sizeof(float));
+            memset(d + ctx->m, 0, (ctx->ldv - ctx->m) * sizeof(float));
+        }
+        e = cudaMemcpyAsync(ctx->dV + (size_t)r0 * ctx->ldv, st, nr * row_bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[c & 1], ctx->stream);
+    }
+    cudaError_t const es = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = es;
+    for (int b = 0; b < 2; b++) {
+        if (ev[b]) cudaEventDestroy(ev[b]);
+        stage_put(stage[b]);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return nmfb_fail(ctx, e == cudaErrorMemoryAllocation ? NMFB_ENOMEM : NMFB_ECUDA, "upload of V: %s",
+                         cudaGetErrorString(e));
+    }
     return NMFB_OK;
 }
 
@@ -264,7 +370,8 @@ static int create_impl(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint3
     if ((rc = dev_alloc(ctx, &ctx->dFirst, kp, "first"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dLastRep, m, "last rep"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dState, 1, "state"))) return rc;
-    NMFB_CUDA_TRY(ctx, cudaMallocHost((void **)&ctx->hState, 2 * sizeof(ConvState)));
+    ctx->hState = (ConvState *)stage_get(2 * sizeof(ConvState));
+    if (!ctx->hState) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked convergence state");
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dTickets, 0, 16 * sizeof(uint32_t), ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dObjTicket, 0, 4 * sizeof(uint32_t), ctx->stream));
     if (ctx->dV) NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dV, 0, (size_t)n * ctx->ldv * sizeof(float), ctx->stream));
@@ -371,9 +478,7 @@ int nmfb_set_V(nmfb_ctx *ctx, const float *V, size_t ldv)
         ctx->v_set = 1;
         return NMFB_OK;
     }
-    NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), V, ldv * sizeof(float),
-                                         ctx->m * sizeof(float), ctx->n, cudaMemcpyHostToDevice, ctx->stream));
-    NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((rc = upload_V(ctx, V, ldv))) return rc;
     ctx->v_set = 1;
     return NMFB_OK;
 }
@@ -753,6 +858,21 @@ int nmfb_set_wait_limit(nmfb_ctx *ctx, uint64_t ns)
     int rc = check_ctx(ctx);
     if (rc) return rc;
     ctx->wait_ns = (unsigned long long)ns;
+    return NMFB_OK;
+}
+
+int nmfb_set_sm_limit(nmfb_ctx *ctx, uint32_t sms)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    int dev_sms = 0;
+    NMFB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    // The partials were sized for the device's SM count; fewer SMs need fewer.
+    ctx->sm_count = (sms == 0 || sms > (uint32_t)dev_sms) ? dev_sms : (int)sms;
+    if (ctx->blk_exec) {   // the captured block holds launch shapes of the old count
+        NMFB_CUDA_TRY(ctx, cudaGraphExecDestroy(ctx->blk_exec));
+        ctx->blk_exec = nullptr;
+    }
     return NMFB_OK;
 }
 

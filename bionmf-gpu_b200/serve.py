@@ -13,7 +13,9 @@ device memory fits the HBM budget, and runs each on one of two paths:
   iteration or per request;
 * larger requests get their own context on their own CUDA stream (V, W, H
   resident for the whole solve, ``NMF.run``), driven by worker threads (the C
-  ABI releases the interpreter lock, so the contexts' kernels overlap).
+  ABI releases the interpreter lock, so the contexts' kernels overlap);
+  ``sm_limit`` sizes each context's launches for that many SMs, so that
+  several requests' kernels share the GPU side by side.
 
 Both paths sum in a fixed order that depends only on the request's own sizes,
 so a request's result is the same alone and in any mix.  Device memory of
@@ -85,7 +87,7 @@ class Server:
     contexts alone)."""
 
     def __init__(self, budget_bytes: float = 120e9, workers: int = 16, arm: str = "fused", device: int = 0,
-                 batched: bool = False, max_m: int = 256, ctas: int = 4):
+                 batched: bool = False, max_m: int = 256, ctas: int = 4, sm_limit: int = 0):
         self.budget = int(budget_bytes)
         self.workers = int(workers)
         self.arm = arm
@@ -93,6 +95,7 @@ class Server:
         self.batched = batched
         self.max_m = int(max_m)
         self.ctas = int(ctas)
+        self.sm_limit = int(sm_limit)   # SMs each context sizes its launches for (0: all)
 
     def _arm_for(self, k: int) -> str:
         return self.arm if k <= 64 else "plain"
@@ -106,9 +109,12 @@ class Server:
             return Serve.request_bytes(n, m, r.k)
         return context_bytes(n, m, r.k, self._arm_for(r.k), self.device)
 
-    def _solve(self, req: Request, t0: float, admitted: float) -> Result:
+    def _solve(self, req: Request, t0: float, admitted: float, sm_limit: int | None = None) -> Result:
         n, m = req.V.shape
+        sm_limit = self.sm_limit if sm_limit is None else sm_limit
         with NMF(n, m, req.k, arm=self._arm_for(req.k), device=self.device) as e:
+            if sm_limit:
+                e.set_sm_limit(sm_limit)
             e.set_V(req.V)
             e.init_random(req.seed)
             it, conv = e.run(req.n_iters, req.niter_test_conv, req.stop_threshold)
@@ -227,12 +233,13 @@ class Server:
         return stats
 
     def run_sequential(self, requests: list[Request]) -> ServeStats:
-        """The baseline: one request at a time, each through its own context."""
+        """The baseline: one request at a time, each through its own context
+        sized for the whole device (sm_limit does not apply)."""
         stats = ServeStats()
         t0 = time.perf_counter()
         for r in sorted(requests, key=lambda r: r.arrival):
             res = self._solve(Request(r.V, r.k, r.seed, r.n_iters, r.niter_test_conv, r.stop_threshold, 0.0, r.rid),
-                              t0, time.perf_counter() - t0)
+                              t0, time.perf_counter() - t0, sm_limit=0)
             stats.results.append(res)
         stats.wall_s = time.perf_counter() - t0
         return stats

@@ -199,6 +199,15 @@ uint64_t nmfb_launch_count(const nmfb_ctx *ctx);
  * on one another. */
 int nmfb_set_wait_limit(nmfb_ctx *ctx, uint64_t ns);
 
+/* Number of SMs this context sizes its launches for (0: all of the device's).
+ * The fused arms split each half-iteration's reduction so that one wave of
+ * CTAs fills that many SMs; a smaller figure leaves room for the kernels of
+ * other contexts on other streams (many small solves served side by side)
+ * and gives each CTA a longer run of tiles.  The split count, and with it the
+ * summation order, depends on this figure and the sizes only.  No counterpart
+ * in the reference, which runs one factorisation per process. */
+int nmfb_set_sm_limit(nmfb_ctx *ctx, uint32_t sms);
+
 /* ---------------------------------------------------------------------------
  * Batched solves: rank-selection and restart sweeps.  The reference runs one
  * factorisation per process (nmf(), src/NMF_GPU.c:522-795; its user guide,

@@ -56,6 +56,23 @@ def test_results_same_alone_and_in_the_mix(pkg, synth, batched):
             assert np.array_equal(r.W, seq[r.rid].W) and np.array_equal(r.H, seq[r.rid].H)
 
 
+def test_sm_limit_same_alone_and_in_the_mix(pkg, synth):
+    """Contexts sized for 37 SMs: a request's result is the same alone and in
+    the mix, and within FP32 summation-order noise of the whole-device run."""
+    import nmf_b200.serve as serve
+
+    reqs = _requests(synth, count=8, seed=2)
+    srv = serve.Server(budget_bytes=40e9, workers=6, sm_limit=37)
+    alone = {r.rid: srv.run([r], open_loop=False).results[0] for r in reqs}
+    mixed = srv.run(reqs, open_loop=True)
+    full = {r.rid: r for r in srv.run_sequential(reqs).results}
+    assert mixed.peak_active > 1
+    for r in mixed.results:
+        a, f = alone[r.rid], full[r.rid]
+        assert np.array_equal(r.W, a.W) and np.array_equal(r.H, a.H)
+        assert maxnorm_rel(r.W, f.W) < 1e-4 and maxnorm_rel(r.H, f.H) < 1e-4
+
+
 def test_admission_respects_the_budget(pkg, synth):
     import nmf_b200.serve as serve
 
