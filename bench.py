@@ -632,9 +632,9 @@ def serve_small_rates(dev, seq_sample=40):
                      batched=True)
     c = serve.Server(budget_bytes=SERVE["budget_gb"] * 1e9, workers=SERVE["workers"], device=dev.index or 0,
                      sm_limit=SERVE["sm_limit"])
-    q.run(reqs[:8], open_loop=False)
-    c.run(reqs[:8], open_loop=False)
+    q.run(reqs[:8], open_loop=False)                  # each path warmed up right before its own run
     qs = q.run(reqs, open_loop=False)
+    c.run(reqs[:8], open_loop=False)
     cs = c.run(reqs, open_loop=False)
     seq = c.run_sequential(reqs[:seq_sample])
     return {"workload": SERVE_SMALL["desc"], "requests": len(reqs), "unit": "solves/s",

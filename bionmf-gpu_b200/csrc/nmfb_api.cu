@@ -222,13 +222,21 @@ int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, 
     return NMFB_OK;
 }
 
-// Upload the host matrix V (n x m, ld) into the device's n x ldv layout: rows
-// are packed at the device pitch (padding zero) into two page-locked staging
-// buffers of at most 8 MB in turn, each copied with one DMA while the next is
-// filled.  (A pitched copy straight from pageable memory moves one short row
-// at a time.)
+// Upload the host matrix V (n x m, ld) into the device's n x ldv layout.  From
+// page-locked memory: one pitched DMA.  From pageable memory: rows are packed
+// at the device pitch (padding zero) into two page-locked staging buffers of
+// at most 8 MB in turn, each copied with one DMA while the next is filled (a
+// pitched copy straight from pageable memory moves one short row at a time).
 int upload_V(nmfb_ctx *ctx, const float *V, size_t ld)
 {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, V) == cudaSuccess && pa.type == cudaMemoryTypeHost) {
+        NMFB_CUDA_TRY(ctx, cudaMemcpy2DAsync(ctx->dV, ctx->ldv * sizeof(float), V, ld * sizeof(float),
+                                             ctx->m * sizeof(float), ctx->n, cudaMemcpyHostToDevice, ctx->stream));
+        NMFB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        return NMFB_OK;
+    }
+    cudaGetLastError();
     size_t const row_bytes = ctx->ldv * sizeof(float);
     uint32_t const per = (uint32_t)((size_t)(8u << 20) / row_bytes > 0 ? (size_t)(8u << 20) / row_bytes : 1);
     uint32_t const rows = per < ctx->n ? per : ctx->n;
