@@ -85,10 +85,13 @@ int nmfb_create_streamed(nmfb_ctx **ctx, int device, uint32_t n, uint32_t m, uin
 uint64_t nmfb_context_bytes(int device, uint32_t n, uint32_t m, uint32_t k, int arm, uint32_t stream_rows);
 
 /* Context device memory comes from a library-owned stream-ordered pool per
- * device (cudaMallocFromPoolAsync), so contexts can be created and destroyed
- * while others compute without synchronising the device.  Freed memory stays
- * cached in the pool for the next context; this returns it to the driver
- * (after synchronising the device).  No counterpart in the reference. */
+ * device (cudaMallocFromPoolAsync), and page-locked host staging buffers (for
+ * uploads and downloads, up to 8 MB each, one or two per call in flight) from
+ * a process-wide pool, so contexts can be created, fed and destroyed while
+ * others compute without synchronising the device.  Freed memory stays
+ * cached in the pools for the next context; this returns the device pool's
+ * memory to the driver (after synchronising the device) and frees the
+ * staging buffers no call holds.  No counterpart in the reference. */
 int nmfb_release_cached(int device);
 
 /* finalize_GPU_device (src/GPU_setup.c:2291): frees everything. NULL is a no-op. */
