@@ -17,6 +17,14 @@ using nmfb_tc::BO;
 using nmfb_tc::tf32_rna;
 
 constexpr uint32_t FIN_ECH = 32;   // row blocks per chunk of k_finish's column sums
+constexpr uint32_t FIN_RB = 32;    // rows of X per k_finish CTA
+
+// k_finish's launch shape for a factor of `rows` rows: KP / 4 threads per row,
+// and enough 32-row blocks to cover every 64-row block of the split copies
+// (rows past the end get zeros there).
+template <int KP>
+constexpr int fin_threads() { return (int)FIN_RB * (KP / 4); }
+inline uint32_t fin_blocks(uint32_t rows) { return 2u * ((rows + 63u) / 64u); }
 
 // Two floats to a BF16 pair (round to nearest even), `first` in the low half.
 __device__ __forceinline__ uint32_t fin_bf16x2(float first, float second)
@@ -26,19 +34,22 @@ __device__ __forceinline__ uint32_t fin_bf16x2(float first, float second)
     return r;
 }
 
-// Finish of a half-iteration, one CTA of 512 threads per 128-row block of X
-// (four threads per row, a quarter of its columns each), right after the fused
-// kernel (k_fused_half, LAYOUT 0, or k_fused_bf16, LAYOUT 1):
+// Finish of a half-iteration, one CTA per FIN_RB = 32 rows of X, KP / 4 threads
+// per row (four consecutive columns each), right after the fused kernel
+// (k_fused_half, LAYOUT 0, or k_fused_bf16, LAYOUT 1):
 //   Xaux = the split partials summed in split order; X = X * Xaux / accY
 //   (matrix_mul_div, src/GPU_kernels.cu:1885-2058: product first, then the
 //   division, correctly rounded) with the EPS adjust when asked (kernel_adjust,
 //   :2338-2345); then X's split copies in the arm's layout (LAYOUT 0:
 //   k_split_factor's, LAYOUT 1: k_split_bf16's) and its column
 //   sums (matrix_to_row, src/GPU_kernels.cu:871-1066) in FP64: a shuffle tree over
-//   each warp's 8 rows, the 16 warps in order, row blocks in chunks of FIN_ECH in block order,
-//   the chunks in order -- fixed orders throughout, so the result does not depend
-//   on scheduling.  It replaces the reference's mul_div + adjust and, for the next
-//   half-iteration, its column sums, in one launch.
+//   each warp's rows, the warps in order, row blocks in chunks of FIN_ECH in block
+//   order, the chunks in order -- fixed orders throughout, so the result does not
+//   depend on scheduling.  It replaces the reference's mul_div + adjust and, for the
+//   next half-iteration, its column sums, in one launch.  Small blocks and the
+//   partials of up to eight splits in flight per thread keep each CTA's chain of
+//   dependent memory round trips short: the kernel is latency-bound, its traffic
+//   (the partials, X and its copies) small.
 struct FinishArgs {
     uint32_t O, nsplit, k;
     int adjust;
@@ -58,161 +69,141 @@ struct FinishArgs {
 };
 
 template <int KP, int BR, int LAYOUT>
-__global__ void __launch_bounds__(512) k_finish(const FinishArgs a)
+__global__ void __launch_bounds__(FIN_RB * KP / 4) k_finish(const FinishArgs a)
 {
-    constexpr int CPT = KP / 4;          // columns per thread (4 threads per row)
-    constexpr int NW = 16;               // warps
+    constexpr int TPR = KP / 4;                  // threads per row
+    constexpr int NT = (int)FIN_RB * TPR;        // 128 / 256 / 512 threads for KP = 16 / 32 / 64
+    constexpr int NW = NT / 32;                  // warps
+    constexpr int QB = 8;                        // split partials in flight per thread
+    static_assert(32 % TPR == 0 && NT % KP == 0, "k_finish shape");
     if (a.st && *(volatile const uint32_t *)&a.st->converged) return;
-    __shared__ double ws[NW * KP + 512];
+    __shared__ double ws[NW * KP + NT];
     __shared__ uint32_t eflag;
     uint32_t const tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
-    uint32_t const row = tid / 4, c0 = (tid % 4) * CPT;
-    uint32_t const oblk = blockIdx.x, nob = gridDim.x;
-    uint32_t const o = oblk * BO + row;
+    uint32_t const row = tid / TPR, c0 = (tid % TPR) * 4;
+    uint32_t const blk = blockIdx.x, nob = gridDim.x;
+    uint32_t const o = blk * FIN_RB + row;
     bool const in = o < a.O;
-    float x[CPT];
-#pragma unroll
-    for (int c = 0; c < CPT; c++) x[c] = 0.0f;
+    float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if (in) {
-        // Xaux: the split partials in split order, loads issued four splits at a time
+        float *xr = a.X + (size_t)o * KP + c0;
+        float4 const xv = *reinterpret_cast<const float4 *>(xr);    // independent of the partials
+        // Xaux: the split partials in split order, QB loads in flight at a time
         const float *pr = a.part + (size_t)o * KP + c0;
         size_t const qs = (size_t)a.O * KP;
-        uint32_t q = 0;
-        for (; q + 4 <= a.nsplit; q += 4) {
-            float4 v[4][CPT / 4];
+        for (uint32_t q = 0; q < a.nsplit; q += QB) {
+            float4 v[QB];
 #pragma unroll
-            for (int j = 0; j < 4; j++)
+            for (int j = 0; j < QB; j++)
+                v[j] = (q + j < a.nsplit) ? __ldcg(reinterpret_cast<const float4 *>(pr + (q + j) * qs))
+                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-                for (int c = 0; c < CPT / 4; c++) v[j][c] = __ldcg(reinterpret_cast<const float4 *>(pr + (q + j) * qs) + c);
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-#pragma unroll
-                for (int c = 0; c < CPT / 4; c++) {
-                    x[4 * c] += v[j][c].x;
-                    x[4 * c + 1] += v[j][c].y;
-                    x[4 * c + 2] += v[j][c].z;
-                    x[4 * c + 3] += v[j][c].w;
+            for (int j = 0; j < QB; j++)
+                if (q + j < a.nsplit) {
+                    x[0] += v[j].x;
+                    x[1] += v[j].y;
+                    x[2] += v[j].z;
+                    x[3] += v[j].w;
                 }
         }
-        for (; q < a.nsplit; q++) {
+        float const xs[4] = {xv.x, xv.y, xv.z, xv.w};
 #pragma unroll
-            for (int c = 0; c < CPT / 4; c++) {
-                float4 const v = __ldcg(reinterpret_cast<const float4 *>(pr + q * qs) + c);
-                x[4 * c] += v.x;
-                x[4 * c + 1] += v.y;
-                x[4 * c + 2] += v.z;
-                x[4 * c + 3] += v.w;
+        for (int i = 0; i < 4; i++) {
+            uint32_t const cc = c0 + i;
+            float v = 0.0f;
+            if (cc < a.k) {
+                v = __fdiv_rn(xs[i] * x[i], __ldg(a.accY + cc));
+                if (a.adjust) v = fmaxf(v, FLT_MIN);
             }
+            x[i] = v;
         }
-        float *xr = a.X + (size_t)o * KP + c0;
-#pragma unroll
-        for (int c = 0; c < CPT; c += 4) {
-            float4 const xv = *reinterpret_cast<const float4 *>(xr + c);
-            float const xs[4] = {xv.x, xv.y, xv.z, xv.w};
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                uint32_t const cc = c0 + c + i;
-                float v = 0.0f;
-                if (cc < a.k) {
-                    v = __fdiv_rn(xs[i] * x[c + i], __ldg(a.accY + cc));
-                    if (a.adjust) v = fmaxf(v, FLT_MIN);
-                }
-                x[c + i] = v;
-            }
-            *reinterpret_cast<float4 *>(xr + c) = make_float4(x[c], x[c + 1], x[c + 2], x[c + 3]);
-        }
+        *reinterpret_cast<float4 *>(xr) = make_float4(x[0], x[1], x[2], x[3]);
     }
     // split copies; rows past the end are zero in the transposed blocks that exist
     if (LAYOUT == 0) {
         uint32_t const b32 = o / 32, bbr = o / BR;
         bool const tin = b32 < a.xnblk32, btin = bbr < a.xnblkbr;
-        float *T32 = a.xT + (size_t)b32 * 2 * KP * 32 + (o % 32);
-        __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + (o % BR);
+        float h[4], l[4];
 #pragma unroll
-        for (int c = 0; c < CPT; c += 4) {
-            float h[4], l[4];
+        for (int i = 0; i < 4; i++) {
+            h[i] = tf32_rna(x[i]);
+            l[i] = x[i] - h[i];
+        }
+        if (in) {
+            size_t const e = (size_t)o * KP + c0;
+            *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(fin_bf16x2(l[0], l[1]), fin_bf16x2(l[2], l[3]));
+            *reinterpret_cast<uint2 *>(a.xB + e) = make_uint2(fin_bf16x2(x[0], x[1]), fin_bf16x2(x[2], x[3]));
+        }
+        if (tin) {
+            float *T32 = a.xT + (size_t)b32 * 2 * KP * 32 + (o % 32);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                h[i] = tf32_rna(x[c + i]);
-                l[i] = x[c + i] - h[i];
+                T32[(c0 + i) * 32] = h[i];
+                T32[(KP + c0 + i) * 32] = l[i];
             }
-            if (in) {
-                size_t const e = (size_t)o * KP + c0 + c;
-                *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(fin_bf16x2(l[0], l[1]), fin_bf16x2(l[2], l[3]));
-                *reinterpret_cast<uint2 *>(a.xB + e) = make_uint2(fin_bf16x2(x[c], x[c + 1]), fin_bf16x2(x[c + 2], x[c + 3]));
-            }
-            if (tin) {
+        }
+        if (btin) {
+            __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + (o % BR);
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    T32[(c0 + c + i) * 32] = h[i];
-                    T32[(KP + c0 + c + i) * 32] = l[i];
-                }
-            }
-            if (btin) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) BT[(c0 + c + i) * BR] = __float2bfloat16_rn(x[c + i]);
-            }
+            for (int i = 0; i < 4; i++) BT[(c0 + i) * BR] = __float2bfloat16_rn(x[i]);
         }
     } else {
         // hi = bf16(x), lo = bf16(x - hi), both rounded to nearest (k_split_bf16)
         uint32_t const b64 = o / 64;
         bool const tin = b64 < a.bnblk64;
-        __nv_bfloat16 *T64 = a.bT + (size_t)b64 * 2 * KP * 64 + (o % 64);
+        __nv_bfloat16 h[4], l[4];
 #pragma unroll
-        for (int c = 0; c < CPT; c += 4) {
-            __nv_bfloat16 h[4], l[4];
+        for (int i = 0; i < 4; i++) {
+            h[i] = __float2bfloat16_rn(x[i]);
+            l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
+        }
+        if (in) {
+            size_t const e = (size_t)o * KP + c0;
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                h[i] = __float2bfloat16_rn(x[c + i]);
-                l[i] = __float2bfloat16_rn(x[c + i] - __bfloat162float(h[i]));
+                a.bhi[e + i] = h[i];
+                a.blo[e + i] = l[i];
             }
-            if (in) {
-                size_t const e = (size_t)o * KP + c0 + c;
+        }
+        if (tin) {
+            __nv_bfloat16 *T64 = a.bT + (size_t)b64 * 2 * KP * 64 + (o % 64);
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    a.bhi[e + i] = h[i];
-                    a.blo[e + i] = l[i];
-                }
-            }
-            if (tin) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    T64[(c0 + c + i) * 64] = h[i];
-                    T64[(KP + c0 + c + i) * 64] = l[i];
-                }
+            for (int i = 0; i < 4; i++) {
+                T64[(c0 + i) * 64] = h[i];
+                T64[(KP + c0 + i) * 64] = l[i];
             }
         }
     }
-    // column sums of this row block: the warp's 8 rows of each column by a shuffle
-    // tree (lanes 4r + g hold row r, column group g), then the 16 warps in order
+    // column sums of this row block: the warp's rows of each column by a shuffle
+    // tree (lane TPR r + g holds row r, column group g), then the warps in order
 #pragma unroll
-    for (int c = 0; c < CPT; c++) {
+    for (int c = 0; c < 4; c++) {
         double v = (double)x[c];
 #pragma unroll
-        for (int off = 16; off >= 4; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane < 4) ws[warp * KP + c0 + c] = v;
+        for (int off = 16; off >= TPR; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane < (uint32_t)TPR) ws[warp * KP + c0 + c] = v;
     }
     __syncthreads();
     if (tid < (uint32_t)KP) {
         double t = 0.0;
 #pragma unroll
         for (int w = 0; w < NW; w++) t += ws[w * KP + tid];
-        a.cs[(size_t)oblk * KP + tid] = t;
+        a.cs[(size_t)blk * KP + tid] = t;
     }
     __threadfence();
     __syncthreads();
-    uint32_t const nch = (nob + FIN_ECH - 1) / FIN_ECH, ch = oblk / FIN_ECH;
+    uint32_t const nch = (nob + FIN_ECH - 1) / FIN_ECH, ch = blk / FIN_ECH;
     uint32_t const b0 = ch * FIN_ECH, bn = min(nob - b0, FIN_ECH);
     if (tid == 0) eflag = (atomicAdd(&a.tick[ch], 1u) == bn - 1) ? 1u : 0u;
     __syncthreads();
     if (!eflag) return;
     // last row block of its chunk: the chunk's partials in block order
     __threadfence();
-    constexpr int GRP = 512 / KP;
+    constexpr int GRP = NT / KP;
     uint32_t const g = tid / KP, c = tid % KP;
     double t = 0.0;
-    for (uint32_t blk = g; blk < bn; blk += GRP) t += __ldcg(a.cs + (size_t)(b0 + blk) * KP + c);
+    for (uint32_t b = g; b < bn; b += GRP) t += __ldcg(a.cs + (size_t)(b0 + b) * KP + c);
     ws[NW * KP + tid] = t;
     __syncthreads();
     if (tid < (uint32_t)KP) {

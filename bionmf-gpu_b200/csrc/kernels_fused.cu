@@ -24,7 +24,7 @@
 //              + bf16(Rl) bf16(Y) into Acc[0:KP]               (kind::f16, K = 16).
 //   epilogue : adds Acc[tile] into FP32 registers (per-tile accumulation keeps
 //              the tensor core's FP32 sums short) and writes the split's
-//              partial; k_finish (one CTA per 128 rows) sums the splits, applies
+//              partial; k_finish (one CTA per 32 rows) sums the splits, applies
 //              X = X .* Xaux ./ colsum(Y) (and the EPS adjust when asked), and
 //              writes X's split copies and column sums for the next
 //              half-iteration: two launches per half-iteration.
@@ -822,9 +822,10 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
     fa.accX = HSIDE ? ctx->dAccH : ctx->dAccW;
     fa.tick = plan->dTick;
     fa.st = ctx->dState;
-    if (oblocks > plan->csoff || (oblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
+    uint32_t const fblocks = fin_blocks(O);
+    if (fblocks > plan->csoff || (fblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
         return nmfb_fail(ctx, NMFB_EINVAL, "fused: column-sum buffers too small");
-    k_finish<KP, BR, 0><<<oblocks, 512, 0, ctx->stream>>>(fa);
+    k_finish<KP, BR, 0><<<fblocks, fin_threads<KP>(), 0, ctx->stream>>>(fa);
     NMFB_LAUNCH_CHECK(ctx);
     return (int)nsplit;
 }
@@ -920,7 +921,7 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     uint32_t const br = LW.br;
     e = nmfb_malloc(ctx, (void **)&plan->dSplitW, LW.floats * sizeof(float));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, LH.floats * sizeof(float));
-    uint32_t const maxblk = ((ctx->n > ctx->m ? ctx->n : ctx->m) + BO - 1) / BO;
+    uint32_t const maxblk = fin_blocks(ctx->n > ctx->m ? ctx->n : ctx->m);   // k_finish's row blocks
     plan->csoff = maxblk;
     plan->nticks = (maxblk + FIN_ECH - 1) / FIN_ECH + 1;
     if (e == cudaSuccess)
