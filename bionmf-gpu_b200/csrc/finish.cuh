@@ -19,12 +19,19 @@ using nmfb_tc::tf32_rna;
 constexpr uint32_t FIN_ECH = 32;   // row blocks per chunk of k_finish's column sums
 constexpr uint32_t FIN_RB = 32;    // rows of X per k_finish CTA
 
-// k_finish's launch shape for a factor of `rows` rows: KP / 4 threads per row,
-// and enough 32-row blocks to cover every 64-row block of the split copies
-// (rows past the end get zeros there).
+// k_finish's launch shape for a factor of `rows` rows: KP / 4 threads per row
+// of a 32-row set, RPT row sets per CTA (each thread takes one row of each),
+// and enough CTAs to cover every 64-row block of the split copies (rows past
+// the end get zeros there).  RPT > 1 when there are few splits: more loads in
+// flight per thread, fewer waves of CTAs.
 template <int KP>
 constexpr int fin_threads() { return (int)FIN_RB * (KP / 4); }
-inline uint32_t fin_blocks(uint32_t rows) { return 2u * ((rows + 63u) / 64u); }
+inline uint32_t fin_rpt(uint32_t nsplit) { return nsplit <= 2 ? 4u : nsplit <= 4 ? 2u : 1u; }
+inline uint32_t fin_blocks(uint32_t rows, uint32_t rpt)
+{
+    uint32_t const rows64 = (rows + 63u) / 64u * 64u;
+    return (rows64 + FIN_RB * rpt - 1) / (FIN_RB * rpt);
+}
 
 // Two floats to a BF16 pair (round to nearest even), `first` in the low half.
 __device__ __forceinline__ uint32_t fin_bf16x2(float first, float second)
@@ -68,118 +75,142 @@ struct FinishArgs {
     const ConvState *st;
 };
 
-template <int KP, int BR, int LAYOUT>
+template <int KP, int BR, int LAYOUT, int RPT>
 __global__ void __launch_bounds__(FIN_RB * KP / 4) k_finish(const FinishArgs a)
 {
     constexpr int TPR = KP / 4;                  // threads per row
     constexpr int NT = (int)FIN_RB * TPR;        // 128 / 256 / 512 threads for KP = 16 / 32 / 64
     constexpr int NW = NT / 32;                  // warps
-    constexpr int QB = 8;                        // split partials in flight per thread
-    static_assert(32 % TPR == 0 && NT % KP == 0, "k_finish shape");
+    constexpr int QB = 8 / RPT;                  // splits per row in flight (8 loads per thread)
+    static_assert(32 % TPR == 0 && NT % KP == 0 && QB >= 1, "k_finish shape");
     if (a.st && *(volatile const uint32_t *)&a.st->converged) return;
     __shared__ double ws[NW * KP + NT];
+    __shared__ float sx[KP * 33];                // x of one 32-row set, column-major (padded)
     __shared__ uint32_t eflag;
     uint32_t const tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     uint32_t const row = tid / TPR, c0 = (tid % TPR) * 4;
     uint32_t const blk = blockIdx.x, nob = gridDim.x;
-    uint32_t const o = blk * FIN_RB + row;
-    bool const in = o < a.O;
-    float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    if (in) {
-        float *xr = a.X + (size_t)o * KP + c0;
-        float4 const xv = *reinterpret_cast<const float4 *>(xr);    // independent of the partials
-        // Xaux: the split partials in split order, QB loads in flight at a time
-        const float *pr = a.part + (size_t)o * KP + c0;
-        size_t const qs = (size_t)a.O * KP;
-        for (uint32_t q = 0; q < a.nsplit; q += QB) {
-            float4 v[QB];
+    size_t const qs = (size_t)a.O * KP;
+    // this thread's rows: one in each 32-row set of the CTA's block
+    uint32_t o[RPT];
+    bool in[RPT];
+    float x[RPT][4];
+    float4 xv[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        o[r] = (blk * RPT + r) * FIN_RB + row;
+        in[r] = o[r] < a.O;
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[r][i] = 0.0f;
+        xv[r] = in[r] ? *reinterpret_cast<const float4 *>(a.X + (size_t)o[r] * KP + c0)   // independent of the partials
+                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    // Xaux: each row's split partials in split order, QB splits of every row in flight
+    for (uint32_t q = 0; q < a.nsplit; q += QB) {
+        float4 v[RPT][QB];
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
 #pragma unroll
             for (int j = 0; j < QB; j++)
-                v[j] = (q + j < a.nsplit) ? __ldcg(reinterpret_cast<const float4 *>(pr + (q + j) * qs))
-                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                v[r][j] = (in[r] && q + j < a.nsplit)
+                              ? __ldcg(reinterpret_cast<const float4 *>(a.part + (size_t)o[r] * KP + c0 + (q + j) * qs))
+                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
 #pragma unroll
             for (int j = 0; j < QB; j++)
                 if (q + j < a.nsplit) {
-                    x[0] += v[j].x;
-                    x[1] += v[j].y;
-                    x[2] += v[j].z;
-                    x[3] += v[j].w;
+                    x[r][0] += v[r][j].x;
+                    x[r][1] += v[r][j].y;
+                    x[r][2] += v[r][j].z;
+                    x[r][3] += v[r][j].w;
+                }
+    }
+    double csum[4] = {0.0, 0.0, 0.0, 0.0};   // this thread's rows of its columns, in row-set order
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        if (in[r]) {
+            float const xs[4] = {xv[r].x, xv[r].y, xv[r].z, xv[r].w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                uint32_t const cc = c0 + i;
+                float v = 0.0f;
+                if (cc < a.k) {
+                    v = __fdiv_rn(xs[i] * x[r][i], __ldg(a.accY + cc));
+                    if (a.adjust) v = fmaxf(v, FLT_MIN);
+                }
+                x[r][i] = v;
+            }
+            *reinterpret_cast<float4 *>(a.X + (size_t)o[r] * KP + c0) = make_float4(x[r][0], x[r][1], x[r][2], x[r][3]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) csum[i] += (double)x[r][i];
+        // split copies: the row-major ones straight from registers; the transposed
+        // blocks through shared memory (x of the 32-row set, column-major), so that
+        // every store below covers 64-128 contiguous bytes.  Rows past the end are
+        // zero in the transposed blocks that exist.
+        if (LAYOUT == 0) {
+            if (in[r]) {
+                float h[4], l[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    h[i] = tf32_rna(x[r][i]);
+                    l[i] = x[r][i] - h[i];
+                }
+                size_t const e = (size_t)o[r] * KP + c0;
+                *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(fin_bf16x2(l[0], l[1]), fin_bf16x2(l[2], l[3]));
+                *reinterpret_cast<uint2 *>(a.xB + e) =
+                    make_uint2(fin_bf16x2(x[r][0], x[r][1]), fin_bf16x2(x[r][2], x[r][3]));
+            }
+        } else if (in[r]) {
+            // hi = bf16(x), lo = bf16(x - hi), both rounded to nearest (k_split_bf16)
+            size_t const e = (size_t)o[r] * KP + c0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                __nv_bfloat16 const h = __float2bfloat16_rn(x[r][i]);
+                a.bhi[e + i] = h;
+                a.blo[e + i] = __float2bfloat16_rn(x[r][i] - __bfloat162float(h));
+            }
+        }
+        __syncthreads();   // the previous row set's readers of sx are done
+#pragma unroll
+        for (int i = 0; i < 4; i++) sx[(c0 + i) * 33 + row] = x[r][i];
+        __syncthreads();
+        uint32_t const set0 = (blk * RPT + r) * FIN_RB;   // first row of this set
+        if (LAYOUT == 0) {
+            uint32_t const b32 = set0 / 32, bbr = set0 / BR;
+            float *T32 = a.xT + (size_t)b32 * 2 * KP * 32;
+            __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + set0 % BR;
+            for (uint32_t e = tid; e < (uint32_t)KP * 32; e += NT) {
+                uint32_t const c = e / 32, t = e % 32;
+                float const v = sx[c * 33 + t];
+                float const h = tf32_rna(v);
+                if (b32 < a.xnblk32) {
+                    T32[c * 32 + t] = h;
+                    T32[(KP + c) * 32 + t] = v - h;
+                }
+                if (bbr < a.xnblkbr) BT[(size_t)c * BR + t] = __float2bfloat16_rn(v);
+            }
+        } else {
+            uint32_t const b64 = set0 / 64;
+            __nv_bfloat16 *T64 = a.bT + (size_t)b64 * 2 * KP * 64 + set0 % 64;
+            if (b64 < a.bnblk64)
+                for (uint32_t e = tid; e < (uint32_t)KP * 32; e += NT) {
+                    uint32_t const c = e / 32, t = e % 32;
+                    float const v = sx[c * 33 + t];
+                    __nv_bfloat16 const h = __float2bfloat16_rn(v);
+                    T64[(size_t)c * 64 + t] = h;
+                    T64[(size_t)(KP + c) * 64 + t] = __float2bfloat16_rn(v - __bfloat162float(h));
                 }
         }
-        float const xs[4] = {xv.x, xv.y, xv.z, xv.w};
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            uint32_t const cc = c0 + i;
-            float v = 0.0f;
-            if (cc < a.k) {
-                v = __fdiv_rn(xs[i] * x[i], __ldg(a.accY + cc));
-                if (a.adjust) v = fmaxf(v, FLT_MIN);
-            }
-            x[i] = v;
-        }
-        *reinterpret_cast<float4 *>(xr) = make_float4(x[0], x[1], x[2], x[3]);
     }
-    // split copies; rows past the end are zero in the transposed blocks that exist
-    if (LAYOUT == 0) {
-        uint32_t const b32 = o / 32, bbr = o / BR;
-        bool const tin = b32 < a.xnblk32, btin = bbr < a.xnblkbr;
-        float h[4], l[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            h[i] = tf32_rna(x[i]);
-            l[i] = x[i] - h[i];
-        }
-        if (in) {
-            size_t const e = (size_t)o * KP + c0;
-            *reinterpret_cast<float4 *>(a.xhi + e) = make_float4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint2 *>(a.xBl + e) = make_uint2(fin_bf16x2(l[0], l[1]), fin_bf16x2(l[2], l[3]));
-            *reinterpret_cast<uint2 *>(a.xB + e) = make_uint2(fin_bf16x2(x[0], x[1]), fin_bf16x2(x[2], x[3]));
-        }
-        if (tin) {
-            float *T32 = a.xT + (size_t)b32 * 2 * KP * 32 + (o % 32);
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                T32[(c0 + i) * 32] = h[i];
-                T32[(KP + c0 + i) * 32] = l[i];
-            }
-        }
-        if (btin) {
-            __nv_bfloat16 *BT = a.xBT + (size_t)bbr * KP * BR + (o % BR);
-#pragma unroll
-            for (int i = 0; i < 4; i++) BT[(c0 + i) * BR] = __float2bfloat16_rn(x[i]);
-        }
-    } else {
-        // hi = bf16(x), lo = bf16(x - hi), both rounded to nearest (k_split_bf16)
-        uint32_t const b64 = o / 64;
-        bool const tin = b64 < a.bnblk64;
-        __nv_bfloat16 h[4], l[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            h[i] = __float2bfloat16_rn(x[i]);
-            l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
-        }
-        if (in) {
-            size_t const e = (size_t)o * KP + c0;
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                a.bhi[e + i] = h[i];
-                a.blo[e + i] = l[i];
-            }
-        }
-        if (tin) {
-            __nv_bfloat16 *T64 = a.bT + (size_t)b64 * 2 * KP * 64 + (o % 64);
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                T64[(c0 + i) * 64] = h[i];
-                T64[(KP + c0 + i) * 64] = l[i];
-            }
-        }
-    }
-    // column sums of this row block: the warp's rows of each column by a shuffle
-    // tree (lane TPR r + g holds row r, column group g), then the warps in order
+    // column sums of this row block: each thread's rows (above), the warp's lanes
+    // of each column by a shuffle tree (lane TPR r + g holds row r, column group
+    // g), then the warps in order
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        double v = (double)x[c];
+        double v = csum[c];
 #pragma unroll
         for (int off = 16; off >= TPR; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if (lane < (uint32_t)TPR) ws[warp * KP + c0 + c] = v;
@@ -230,6 +261,20 @@ __global__ void __launch_bounds__(FIN_RB * KP / 4) k_finish(const FinishArgs a)
         a.accX[tid] = (float)u;
     }
     if (tid == 0) a.tick[nch] = 0u;
+}
+
+// k_finish for the factor of a.O rows, with the row sets per thread that its
+// split count calls for (the block count is fin_blocks(a.O, fin_rpt(a.nsplit))).
+template <int KP, int BR, int LAYOUT>
+void fin_launch(const FinishArgs &a, cudaStream_t s)
+{
+    uint32_t const rpt = fin_rpt(a.nsplit), nb = fin_blocks(a.O, rpt);
+    if (rpt == 4)
+        k_finish<KP, BR, LAYOUT, 4><<<nb, fin_threads<KP>(), 0, s>>>(a);
+    else if (rpt == 2)
+        k_finish<KP, BR, LAYOUT, 2><<<nb, fin_threads<KP>(), 0, s>>>(a);
+    else
+        k_finish<KP, BR, LAYOUT, 1><<<nb, fin_threads<KP>(), 0, s>>>(a);
 }
 
 }  // namespace

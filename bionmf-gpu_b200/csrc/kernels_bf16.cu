@@ -699,7 +699,7 @@ int launch_finish_b(nmfb_ctx *ctx, bool is_H, uint32_t nsplit, int adjust)
 {
     PlanB *plan = (PlanB *)ctx->bplan;
     uint32_t const O = is_H ? ctx->m : ctx->n;
-    uint32_t const fblocks = fin_blocks(O);
+    uint32_t const fblocks = fin_blocks(O, fin_rpt(nsplit));
     if (fblocks > plan->csoff || (fblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
         return nmfb_fail(ctx, NMFB_EINVAL, "bf16 arms: column-sum buffers too small");
     __nv_bfloat16 *xs = is_H ? plan->hsplit : plan->wsplit;
@@ -721,7 +721,7 @@ int launch_finish_b(nmfb_ctx *ctx, bool is_H, uint32_t nsplit, int adjust)
     fa.accX = is_H ? ctx->dAccH : ctx->dAccW;
     fa.tick = plan->dTick;
     fa.st = ctx->dState;
-    k_finish<KP, 64, 1><<<fblocks, fin_threads<KP>(), 0, ctx->stream>>>(fa);
+    fin_launch<KP, 64, 1>(fa, ctx->stream);
     NMFB_LAUNCH_CHECK(ctx);
     return NMFB_OK;
 }
@@ -772,7 +772,7 @@ int nmfb_bf16_prepare(nmfb_ctx *ctx)
     size_t const wt = (size_t)((ctx->n + 63) / 64) * 128 * kp, ht = (size_t)((ctx->m + 63) / 64) * 128 * kp;
     cudaError_t e = nmfb_malloc(ctx, (void **)&plan->wsplit, (2 * wsz + wt) * sizeof(__nv_bfloat16));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->hsplit, (2 * hsz + ht) * sizeof(__nv_bfloat16));
-    uint32_t const maxblk = fin_blocks(ctx->n > ctx->m ? ctx->n : ctx->m);   // k_finish's row blocks
+    uint32_t const maxblk = fin_blocks(ctx->n > ctx->m ? ctx->n : ctx->m, 1);   // k_finish's most row blocks
     plan->csoff = maxblk;
     plan->nticks = (maxblk + FIN_ECH - 1) / FIN_ECH + 1;
     if (e == cudaSuccess)

@@ -822,10 +822,10 @@ int launch_fused(nmfb_ctx *ctx, const FusedMaps &maps, int adjust)
     fa.accX = HSIDE ? ctx->dAccH : ctx->dAccW;
     fa.tick = plan->dTick;
     fa.st = ctx->dState;
-    uint32_t const fblocks = fin_blocks(O);
+    uint32_t const fblocks = fin_blocks(O, fin_rpt(nsplit));
     if (fblocks > plan->csoff || (fblocks + FIN_ECH - 1) / FIN_ECH + 1 > plan->nticks)
         return nmfb_fail(ctx, NMFB_EINVAL, "fused: column-sum buffers too small");
-    k_finish<KP, BR, 0><<<fblocks, fin_threads<KP>(), 0, ctx->stream>>>(fa);
+    fin_launch<KP, BR, 0>(fa, ctx->stream);
     NMFB_LAUNCH_CHECK(ctx);
     return (int)nsplit;
 }
@@ -921,7 +921,7 @@ int nmfb_fused_prepare(nmfb_ctx *ctx)
     uint32_t const br = LW.br;
     e = nmfb_malloc(ctx, (void **)&plan->dSplitW, LW.floats * sizeof(float));
     if (e == cudaSuccess) e = nmfb_malloc(ctx, (void **)&plan->dSplitH, LH.floats * sizeof(float));
-    uint32_t const maxblk = fin_blocks(ctx->n > ctx->m ? ctx->n : ctx->m);   // k_finish's row blocks
+    uint32_t const maxblk = fin_blocks(ctx->n > ctx->m ? ctx->n : ctx->m, 1);   // k_finish's most row blocks
     plan->csoff = maxblk;
     plan->nticks = (maxblk + FIN_ECH - 1) / FIN_ECH + 1;
     if (e == cudaSuccess)
