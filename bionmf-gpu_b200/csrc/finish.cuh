@@ -76,7 +76,7 @@ struct FinishArgs {
 };
 
 template <int KP, int BR, int LAYOUT, int RPT>
-__global__ void __launch_bounds__(FIN_RB * KP / 4) k_finish(const FinishArgs a)
+__global__ void __launch_bounds__(FIN_RB * KP / 4, 128 / KP) k_finish(const FinishArgs a)   // <= 64 registers
 {
     constexpr int TPR = KP / 4;                  // threads per row
     constexpr int NT = (int)FIN_RB * TPR;        // 128 / 256 / 512 threads for KP = 16 / 32 / 64
