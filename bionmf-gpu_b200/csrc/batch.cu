@@ -1542,11 +1542,48 @@ int nmfb_serve_submit(nmfb_serve *s, const float *V, size_t ldv, uint32_t n, uin
         cudaGetLastError();
         return sfail(s, NMFB_ENOMEM, "request memory: %s", cudaGetErrorString(e));
     }
-    STRY(s, cudaMemsetAsync(ns.V, 0, (size_t)n * ldp * sizeof(float), s->cstream));
-    STRY(s, cudaMemcpy2DAsync(ns.V, ldp * sizeof(float), V, ldv * sizeof(float), m * sizeof(float), n,
-                              cudaMemcpyDefault, s->cstream));
-    STRY(s, cudaMemcpyAsync(ns.W, W.data(), W.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
-    STRY(s, cudaMemcpyAsync(ns.H, H.data(), H.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+    // The request's V, W and H into its device buffers.  From pageable host memory
+    // V's rows are packed at the device pitch (padding zero) into one of the
+    // library's page-locked staging buffers, W and H behind them, and copied with
+    // one DMA each (a pitched copy from pageable memory moves one short row at a
+    // time); device or page-locked V is copied directly.  The staging buffer is
+    // handed back once the copies are done (end of this call).
+    cudaPointerAttributes pa;
+    bool const pageable = !(cudaPointerGetAttributes(&pa, V) == cudaSuccess &&
+                            (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeHost ||
+                             pa.type == cudaMemoryTypeManaged));
+    cudaGetLastError();
+    size_t const vfl = (size_t)n * ldp;
+    struct StageGuard {
+        float *p;
+        cudaStream_t st;
+        ~StageGuard()
+        {
+            if (p) {
+                cudaStreamSynchronize(st);   // the copies reading it are done
+                nmfb_stage_put(p);
+            }
+        }
+    } stage{pageable ? (float *)nmfb_stage_get((vfl + W.size() + H.size()) * sizeof(float)) : nullptr, s->cstream};
+    if (stage.p) {
+        for (uint32_t i = 0; i < n; i++) {
+            float *d = stage.p + (size_t)i * ldp;
+            memcpy(d, V + (size_t)i * ldv, m * sizeof(float));
+            memset(d + m, 0, (ldp - m) * sizeof(float));
+        }
+        memcpy(stage.p + vfl, W.data(), W.size() * sizeof(float));
+        memcpy(stage.p + vfl + W.size(), H.data(), H.size() * sizeof(float));
+        STRY(s, cudaMemcpyAsync(ns.V, stage.p, vfl * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+        STRY(s, cudaMemcpyAsync(ns.W, stage.p + vfl, W.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+        STRY(s, cudaMemcpyAsync(ns.H, stage.p + vfl + W.size(), H.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                s->cstream));
+    } else {
+        STRY(s, cudaMemsetAsync(ns.V, 0, vfl * sizeof(float), s->cstream));
+        STRY(s, cudaMemcpy2DAsync(ns.V, ldp * sizeof(float), V, ldv * sizeof(float), m * sizeof(float), n,
+                                  cudaMemcpyDefault, s->cstream));
+        STRY(s, cudaMemcpyAsync(ns.W, W.data(), W.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+        STRY(s, cudaMemcpyAsync(ns.H, H.data(), H.size() * sizeof(float), cudaMemcpyHostToDevice, s->cstream));
+    }
     Problem &P = s->hRing[slot];
     memset(&P, 0, sizeof(P));
     P.V = ns.V;
@@ -1567,8 +1604,8 @@ int nmfb_serve_submit(nmfb_serve *s, const float *V, size_t ldv, uint32_t n, uin
     // the new published count follows the request's data on the same stream
     s->hPub[slot] = t + 1u;
     STRY(s, cudaMemcpyAsync(s->dCtl + 32, &s->hPub[slot], sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
-    // the pageable W / H copies have been staged when they return; the staging
-    // vectors may go
+    // the W / H vectors have been copied (into the staging buffer, or by the
+    // pageable copies, which return once staged) and may go
     ns.ticket = t + 1u;
     ns.n = n;
     ns.m = m;

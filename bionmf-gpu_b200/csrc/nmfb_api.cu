@@ -65,7 +65,9 @@ struct StageBuf {
 std::mutex g_stage_mutex;
 std::vector<StageBuf> g_stage;
 
-void *stage_get(size_t bytes)
+}  // namespace
+
+void *nmfb_stage_get(size_t bytes)
 {
     std::lock_guard<std::mutex> lock(g_stage_mutex);
     StageBuf *best = nullptr;
@@ -86,7 +88,7 @@ void *stage_get(size_t bytes)
     return p;
 }
 
-void stage_put(void *p)
+void nmfb_stage_put(void *p)
 {
     if (!p) return;
     std::lock_guard<std::mutex> lock(g_stage_mutex);
@@ -97,6 +99,7 @@ void stage_put(void *p)
         }
 }
 
+namespace {
 // Free the staging buffers no context holds.
 void stage_trim()
 {
@@ -176,7 +179,7 @@ void free_all(nmfb_ctx *ctx)
                     ctx->dFirst,   ctx->dLastRep, ctx->dState};
     for (void *b : bufs)
         if (b) nmfb_free(ctx, b);
-    stage_put(ctx->hState);
+    nmfb_stage_put(ctx->hState);
     nmfb_stream_release(ctx);
     nmfb_bf16_release(ctx);
     nmfb_fused_release(ctx);
@@ -194,7 +197,7 @@ void free_all(nmfb_ctx *ctx)
 int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, uint32_t cols, size_t ld)
 {
     size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
-    float *stage = (float *)stage_get(bytes);
+    float *stage = (float *)nmfb_stage_get(bytes);
     if (!stage) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked staging buffer of %zu bytes", bytes);
     for (uint32_t r = 0; r < rows; r++) {
         float *d = stage + (size_t)r * ctx->kp;
@@ -203,7 +206,7 @@ int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, ui
     }
     cudaError_t e = cudaMemcpyAsync(dst, stage, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    stage_put(stage);
+    nmfb_stage_put(stage);
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "upload: %s", cudaGetErrorString(e));
     return NMFB_OK;
 }
@@ -211,13 +214,13 @@ int upload_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, ui
 int download_factor(nmfb_ctx *ctx, float *dst, const float *src, uint32_t rows, size_t ld)
 {
     size_t const bytes = (size_t)rows * ctx->kp * sizeof(float);
-    float *stage = (float *)stage_get(bytes);
+    float *stage = (float *)nmfb_stage_get(bytes);
     if (!stage) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked staging buffer of %zu bytes", bytes);
     cudaError_t e = cudaMemcpyAsync(stage, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess)
         for (uint32_t r = 0; r < rows; r++) memcpy(dst + (size_t)r * ld, stage + (size_t)r * ctx->kp, ctx->k * sizeof(float));
-    stage_put(stage);
+    nmfb_stage_put(stage);
     if (e != cudaSuccess) return nmfb_fail(ctx, NMFB_ECUDA, "download: %s", cudaGetErrorString(e));
     return NMFB_OK;
 }
@@ -240,7 +243,7 @@ int upload_V(nmfb_ctx *ctx, const float *V, size_t ld)
     size_t const row_bytes = ctx->ldv * sizeof(float);
     uint32_t const per = (uint32_t)((size_t)(8u << 20) / row_bytes > 0 ? (size_t)(8u << 20) / row_bytes : 1);
     uint32_t const rows = per < ctx->n ? per : ctx->n;
-    float *stage[2] = {(float *)stage_get(rows * row_bytes), (float *)stage_get(rows * row_bytes)};
+    float *stage[2] = {(float *)nmfb_stage_get(rows * row_bytes), (float *)nmfb_stage_get(rows * row_bytes)};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaError_t e = (stage[0] && stage[1]) ? cudaSuccess : cudaErrorMemoryAllocation;
     for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
@@ -262,7 +265,7 @@ int upload_V(nmfb_ctx *ctx, const float *V, size_t ld)
     if (e == cudaSuccess) e = es;
     for (int b = 0; b < 2; b++) {
         if (ev[b]) cudaEventDestroy(ev[b]);
-        stage_put(stage[b]);
+        nmfb_stage_put(stage[b]);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -378,7 +381,7 @@ static int create_impl(nmfb_ctx **out, int device, uint32_t n, uint32_t m, uint3
     if ((rc = dev_alloc(ctx, &ctx->dFirst, kp, "first"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dLastRep, m, "last rep"))) return rc;
     if ((rc = dev_alloc(ctx, &ctx->dState, 1, "state"))) return rc;
-    ctx->hState = (ConvState *)stage_get(2 * sizeof(ConvState));
+    ctx->hState = (ConvState *)nmfb_stage_get(2 * sizeof(ConvState));
     if (!ctx->hState) return nmfb_fail(ctx, NMFB_ENOMEM, "page-locked convergence state");
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dTickets, 0, 16 * sizeof(uint32_t), ctx->stream));
     NMFB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dObjTicket, 0, 4 * sizeof(uint32_t), ctx->stream));

@@ -94,6 +94,15 @@ struct nmfb_ctx {
 cudaError_t nmfb_malloc(nmfb_ctx *ctx, void **p, size_t bytes);
 void nmfb_free(nmfb_ctx *ctx, void *p);
 
+// Page-locked host staging buffers shared by the whole process (nmfb_api.cu):
+// allocating or freeing page-locked memory is ordered against every stream of
+// the device, so uploads and downloads take buffers from this pool instead.
+// nmfb_stage_get returns a buffer of at least `bytes` (nullptr if none can be
+// allocated); nmfb_stage_put hands it back once the copies reading or writing
+// it have completed.
+void *nmfb_stage_get(size_t bytes);
+void nmfb_stage_put(void *p);
+
 // ---- error helpers -------------------------------------------------------
 int nmfb_fail(nmfb_ctx *ctx, int code, const char *fmt, ...);
 
