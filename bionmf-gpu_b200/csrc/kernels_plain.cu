@@ -62,17 +62,45 @@ __global__ void __launch_bounds__(256) k_gemm_nt(const float *__restrict__ A, co
 }
 
 // WH = V ./ WH over the n x m region (matrix_div_sub in division mode; the
-// reference uses fdividef, src/GPU_kernels.cu:1687-1695).
+// reference uses fdividef, src/GPU_kernels.cu:1687-1695).  Rows over
+// blockIdx.y, columns in float4 chunks over blockIdx.x (rows start on
+// 128-byte boundaries: ld is a multiple of 32); a ragged tail of m % 4 columns
+// element by element.  Padding columns are neither read nor written.
 __global__ void k_div(const float *__restrict__ V, float *__restrict__ WH, uint32_t n, uint32_t m, size_t ld,
                       const ConvState *st)
 {
     if (halted(st)) return;
-    size_t const total = (size_t)n * m;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        size_t const i = e / m, j = e % m;
-        size_t const o = i * ld + j;
-        WH[o] = __fdividef(V[o], WH[o]);
+    uint32_t const m4 = m / 4;
+    for (uint32_t i = blockIdx.y; i < n; i += gridDim.y) {
+        const float4 *v4 = reinterpret_cast<const float4 *>(V + (size_t)i * ld);
+        float4 *w4 = reinterpret_cast<float4 *>(WH + (size_t)i * ld);
+        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < m4; q += gridDim.x * blockDim.x) {
+            float4 const a = v4[q];
+            float4 b = w4[q];
+            b.x = __fdividef(a.x, b.x);
+            b.y = __fdividef(a.y, b.y);
+            b.z = __fdividef(a.z, b.z);
+            b.w = __fdividef(a.w, b.w);
+            w4[q] = b;
+        }
+        if (blockIdx.x == 0)
+            for (uint32_t j = 4 * m4 + threadIdx.x; j < m; j += blockDim.x) {
+                size_t const o = (size_t)i * ld + j;
+                WH[o] = __fdividef(V[o], WH[o]);
+            }
     }
+}
+
+// Launch shape of k_div for `rows` rows: enough column threads for a row's
+// float4 chunks, rows spread over blockIdx.y up to 64K and ~16 CTAs per SM.
+dim3 div_grid(const nmfb_ctx *ctx, uint32_t rows)
+{
+    uint32_t const gx = (ctx->m / 4 + 255) / 256 > 0 ? (ctx->m / 4 + 255) / 256 : 1;
+    uint32_t gy = (16u * (uint32_t)ctx->sm_count + gx - 1) / gx;
+    if (gy > rows) gy = rows;
+    if (gy > 65535u) gy = 65535u;
+    if (gy == 0) gy = 1;
+    return dim3(gx, gy);
 }
 
 // Out[o][c] = sum_r Q(o, r) * F[r][c] for r in this block's reduction chunk.
@@ -146,7 +174,7 @@ struct RedPlan {
 RedPlan plan_split(nmfb_ctx *ctx, uint32_t nout, uint32_t nred)
 {
     uint32_t const oblocks = (nout + 63) / 64;
-    uint32_t want = (2u * (uint32_t)ctx->sm_count + oblocks - 1) / oblocks;
+    uint32_t want = (8u * (uint32_t)ctx->sm_count + oblocks - 1) / oblocks;   // ~8 CTAs per SM of work
     if (want < 1) want = 1;
     if (want > NMFB_MAX_SPLIT) want = NMFB_MAX_SPLIT;
     uint32_t chunk = (nred + want - 1) / want;
@@ -173,10 +201,7 @@ int plain_half(nmfb_ctx *ctx, bool is_H, int adjust)
     k_gemm_nt<<<g, 256, 0, ctx->stream>>>(ctx->dW, ctx->dH, ctx->dWH, ctx->n, ctx->m, ctx->kp, ctx->ldv, ctx->dState);
     NMFB_LAUNCH_CHECK(ctx);
     // 3. WH = V ./ WH
-    size_t const total = (size_t)ctx->n * ctx->m;
-    unsigned dg = (unsigned)((total + 255) / 256);
-    if (dg > 16u * (unsigned)ctx->sm_count) dg = 16u * (unsigned)ctx->sm_count;
-    k_div<<<dg, 256, 0, ctx->stream>>>(ctx->dV, ctx->dWH, ctx->n, ctx->m, ctx->ldv, ctx->dState);
+    k_div<<<div_grid(ctx, ctx->n), 256, 0, ctx->stream>>>(ctx->dV, ctx->dWH, ctx->n, ctx->m, ctx->ldv, ctx->dState);
     NMFB_LAUNCH_CHECK(ctx);
     // 4. Xaux = Q^T Y (update_H) or Q Y (update_W), split over the reduction.
     RedPlan const p = plan_split(ctx, xrows, yrows);
@@ -206,11 +231,7 @@ int nmfb_plain_wh(nmfb_ctx *ctx, const float *W, uint32_t rows, float *WH)
 
 int nmfb_plain_div(nmfb_ctx *ctx, const float *V, float *WH, uint32_t rows)
 {
-    size_t const total = (size_t)rows * ctx->m;
-    unsigned dg = (unsigned)((total + 255) / 256);
-    if (dg > 16u * (unsigned)ctx->sm_count) dg = 16u * (unsigned)ctx->sm_count;
-    if (dg == 0) dg = 1;
-    k_div<<<dg, 256, 0, ctx->stream>>>(V, WH, rows, ctx->m, ctx->ldv, ctx->dState);
+    k_div<<<div_grid(ctx, rows), 256, 0, ctx->stream>>>(V, WH, rows, ctx->m, ctx->ldv, ctx->dState);
     NMFB_LAUNCH_CHECK(ctx);
     return NMFB_OK;
 }
