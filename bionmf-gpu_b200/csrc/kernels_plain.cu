@@ -205,6 +205,8 @@ int plain_half(nmfb_ctx *ctx, bool is_H, int adjust)
     NMFB_LAUNCH_CHECK(ctx);
     // 4. Xaux = Q^T Y (update_H) or Q Y (update_W), split over the reduction.
     RedPlan const p = plan_split(ctx, xrows, yrows);
+    if ((size_t)p.nsplit * xrows * ctx->kp > ctx->part_items)
+        return nmfb_fail(ctx, NMFB_EINVAL, "partial buffer too small (%u splits of %u rows)", p.nsplit, xrows);
     dim3 rg((xrows + 63) / 64, p.nsplit);
     if ((rc = nmfb_prof_begin(ctx, main))) return rc;
     k_gemm_red<<<rg, 256, 0, ctx->stream>>>(ctx->dWH, ctx->ldv, is_H ? 1 : 0, Y, xrows, yrows, ctx->kp, p.chunk,
